@@ -1,0 +1,196 @@
+"""easybem-b200: B200-native matrix-free Galerkin Laplace layer potentials.
+
+Two Python surfaces over the CUDA library ``libeasybem_gpu.so``:
+
+* the module functions of easybem's pybind module for the GPU path
+  (python/bindings.cpp:186-253): ``init_gpu``, ``close_gpu``,
+  ``apply_gpu_laplace3d_1layer``, ``apply_gpu_laplace3d_1layer_linears``,
+  ``apply_gpu_laplace3d_2layer``, ``apply_gpu_laplace3d_hypersing`` and
+  ``version`` — same names, arguments (1-based elements, the ``order``
+  index, ignored ``nblocks``/``nthreads``) and result sizes, over one
+  process-global mesh;
+* ``Mesh``: a handle-based form with an explicit precision
+  (``"fp64"``, the default, or ``"mixed"``) and device-pointer applies.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from ._lib import EB_PREC_FP64, EB_PREC_MIXED, EasyBemError, check, lib
+
+__all__ = ["Mesh", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
+           "apply_gpu_laplace3d_1layer_linears", "apply_gpu_laplace3d_2layer",
+           "apply_gpu_laplace3d_hypersing", "version", "precision_code"]
+
+
+def precision_code(precision) -> int:
+    if precision in (None, "fp64", "double", EB_PREC_FP64):
+        return EB_PREC_FP64
+    if precision in ("mixed", "fp32", EB_PREC_MIXED):
+        return EB_PREC_MIXED
+    raise ValueError(f"unknown precision {precision!r}: use 'fp64' or 'mixed'")
+
+
+def _vec(a, n, name):
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    if a.shape[0] != n:
+        raise ValueError(f"{name} has {a.shape[0]} entries, expected {n}")
+    return a
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Mesh:
+    """A surface mesh resident on the GPU with its FP64 near-field correction.
+
+    ``nodes``: float [n, 3]; ``elems``: int [m, 3], 1-based (easybem's
+    convention); ``order``: easybem quadrature index (default 4).
+    """
+
+    def __init__(self, nodes, elems, order: int = 4):
+        L = lib()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        elems = np.ascontiguousarray(elems, dtype=np.int32)
+        if nodes.ndim != 2 or nodes.shape[1] != 3 or elems.ndim != 2 or elems.shape[1] != 3:
+            raise ValueError("nodes must be [n, 3] and elements [m, 3]")
+        h = ctypes.c_void_p()
+        check(L.eb_mesh_create(nodes.shape[0], _ptr(nodes), elems.shape[0], _ptr(elems), int(order),
+                               ctypes.byref(h)))
+        self._h = h
+        self.nnodes = nodes.shape[0]
+        self.nelems = elems.shape[0]
+        self.order = order
+        nv, ne, npairs, nquad = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong()
+        check(L.eb_mesh_info(h, ctypes.byref(nv), ctypes.byref(ne), ctypes.byref(npairs), ctypes.byref(nquad)))
+        self.near_pairs = npairs.value
+        self.far_quad_pairs = nquad.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().eb_mesh_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # host-buffer applies -------------------------------------------------
+    def apply_sl(self, t, precision="fp64"):
+        """v = V t (P0 single layer), t and v of length nelems."""
+        t = _vec(t, self.nelems, "t")
+        v = np.empty(self.nelems)
+        check(lib().eb_apply_sl_p0(self._h, precision_code(precision), _ptr(t), _ptr(v)))
+        return v
+
+    def apply_dl(self, u, precision="fp64"):
+        """q = K u (double layer, P0 test x P1 trial), u of length nnodes."""
+        u = _vec(u, self.nnodes, "u")
+        q = np.empty(self.nelems)
+        check(lib().eb_apply_dl_p1(self._h, precision_code(precision), _ptr(u), _ptr(q)))
+        return q
+
+    def apply_sl_dl(self, t, u, precision="fp64"):
+        """(V t, K u) in one pass over the pairs."""
+        t = _vec(t, self.nelems, "t")
+        u = _vec(u, self.nnodes, "u")
+        v = np.empty(self.nelems)
+        q = np.empty(self.nelems)
+        check(lib().eb_apply_sl_dl(self._h, precision_code(precision), _ptr(t), _ptr(u), _ptr(v), _ptr(q)))
+        return v, q
+
+    def apply_sl_p1(self, t, precision="fp64"):
+        """v = V1 t (P1 x P1 single layer), t and v of length nnodes."""
+        t = _vec(t, self.nnodes, "t")
+        v = np.empty(self.nnodes)
+        check(lib().eb_apply_sl_p1(self._h, precision_code(precision), _ptr(t), _ptr(v)))
+        return v
+
+    def apply_hypersingular(self, u, precision="fp64"):
+        """q = D u (hypersingular operator, curl form), u and q of length nnodes."""
+        u = _vec(u, self.nnodes, "u")
+        q = np.empty(self.nnodes)
+        check(lib().eb_apply_hypersingular(self._h, precision_code(precision), _ptr(u), _ptr(q)))
+        return q
+
+    # device-pointer apply ------------------------------------------------
+    def apply_device(self, d_t, d_u, d_v, d_q, precision="fp64", stream=0):
+        """Asynchronous apply on device pointers (ints); 0 skips an operator."""
+        check(lib().eb_apply_sl_dl_device(self._h, precision_code(precision), ctypes.c_void_p(d_t or None),
+                                          ctypes.c_void_p(d_u or None), ctypes.c_void_p(d_v or None),
+                                          ctypes.c_void_p(d_q or None), ctypes.c_void_p(stream or None)))
+
+    def set_profiling(self, on: bool = True):
+        check(lib().eb_set_profiling(self._h, 1 if on else 0))
+
+    def last_kernel_ms(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(lib().eb_last_kernel_ms(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+
+# ---------------------------------------------------------------------------
+# easybem's module-level GPU API (python/bindings.cpp:186-253).
+
+_global_mesh: Mesh | None = None
+
+
+def _legacy_precision():
+    return "mixed" if os.environ.get("EASYBEM_PRECISION", "fp64") in ("mixed", "fp32") else "fp64"
+
+
+def init_gpu(nodes, elements, order: int = 4, nblocks: int = 0, nthreads: int = 0):
+    """Uploads the process-global mesh (``nblocks``/``nthreads`` are ignored)."""
+    global _global_mesh
+    if _global_mesh is not None:
+        _global_mesh.close()
+    _global_mesh = Mesh(nodes, elements, order)
+
+
+def close_gpu():
+    global _global_mesh
+    if _global_mesh is not None:
+        _global_mesh.close()
+    _global_mesh = None
+
+
+def _mesh() -> Mesh:
+    if _global_mesh is None:
+        raise RuntimeError("init_gpu must be called first")
+    return _global_mesh
+
+
+def apply_gpu_laplace3d_1layer(vec):
+    return _mesh().apply_sl(vec, _legacy_precision())
+
+
+def apply_gpu_laplace3d_1layer_linears(vec):
+    return _mesh().apply_sl_p1(vec, _legacy_precision())
+
+
+def apply_gpu_laplace3d_2layer(vec):
+    return _mesh().apply_dl(vec, _legacy_precision())
+
+
+def apply_gpu_laplace3d_hypersing(vec):
+    return _mesh().apply_hypersingular(vec, _legacy_precision())
+
+
+def version():
+    return "1.0"

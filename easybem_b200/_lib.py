@@ -1,0 +1,84 @@
+"""ctypes binding of libeasybem_gpu.so (the C ABI of include/easybem_gpu.h).
+
+The shared library is built in-tree by ``easybem_b200.build``. There is no
+CPU fallback: if the library is missing or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libeasybem_gpu.so")
+
+EB_OK = 0
+EB_ERR_INVALID = 1
+EB_ERR_MESH = 2
+EB_ERR_CUDA = 3
+EB_ERR_NOMEM = 4
+EB_ERR_TIMEOUT = 5
+EB_ERR_STATE = 6
+EB_ERR_NOT_CONVERGED = 7
+
+EB_PREC_FP64 = 0
+EB_PREC_MIXED = 1
+
+_STATUS_NAMES = {1: "invalid argument", 2: "invalid mesh", 3: "CUDA error", 4: "out of memory",
+                 5: "timeout", 6: "bad state", 7: "not converged"}
+
+# name -> (restype, argtypes); every entry point returns an int status except
+# the two string accessors.
+_dp = ctypes.c_void_p
+_SIGNATURES = {
+    "eb_version": (ctypes.c_char_p, []),
+    "eb_last_error": (ctypes.c_char_p, []),
+    "eb_mesh_create": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.POINTER(_dp)]),
+    "eb_mesh_destroy": (ctypes.c_int, [_dp]),
+    "eb_mesh_info": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_apply_sl_p0": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_apply_dl_p1": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_apply_sl_dl": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp, _dp]),
+    "eb_apply_sl_dl_device": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]),
+    "eb_apply_sl_p1": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_apply_hypersingular": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_quadrature": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp,
+                                     ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]),
+    "eb_set_profiling": (ctypes.c_int, [_dp, ctypes.c_int]),
+    "eb_last_kernel_ms": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+}
+
+
+class EasyBemError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"easybem error {status} ({_STATUS_NAMES.get(status, '?')}): {message}")
+        self.status = status
+
+
+_LIB = None
+
+
+def lib():
+    """Loads the CUDA library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m easybem_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            if hasattr(L, name):
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(status: int):
+    if status != EB_OK:
+        raise EasyBemError(status, lib().eb_last_error().decode(errors="replace"))
+
+
+def exported_symbols():
+    """Names declared in include/easybem_gpu.h that the library must export."""
+    return list(_SIGNATURES)

@@ -1,0 +1,489 @@
+// Device-resident mesh, FP64 Sauter-Schwab near field and the apply pipeline
+// (prep -> far field -> finalize), plus the C ABI of include/easybem_gpu.h.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "pairs.h"
+
+namespace eb {
+
+static thread_local std::string g_last_error;
+
+int set_error(int status, const std::string& msg)
+{
+  g_last_error = msg;
+  return status;
+}
+
+const char* last_error() { return g_last_error.c_str(); }
+
+int DevBuf::alloc(size_t n)
+{
+  if (n <= bytes && p) return EB_OK;
+  release();
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    return set_error(e == cudaErrorMemoryAllocation ? EB_ERR_NOMEM : EB_ERR_CUDA,
+                     std::string("cudaMalloc(") + std::to_string(n) + "): " + cudaGetErrorString(e));
+  }
+  bytes = n;
+  return EB_OK;
+}
+
+template <typename T>
+static int upload(DevBuf& b, const std::vector<T>& v)
+{
+  EB_CHECK(b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1)));
+  if (!v.empty()) EB_CUDA(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return EB_OK;
+}
+
+Mesh::~Mesh()
+{
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (ev2) cudaEventDestroy(ev2);
+}
+
+// ---------------------------------------------------------------------------
+// Near field: one thread per near pair computes the FP64 Sauter-Schwab SL
+// value and three DL weights; DL weights landing on the same (row, vertex)
+// are then summed in ascending pair order.
+
+__global__ void near_values_kernel(Quadrature q, const double* __restrict__ nodes, const int* __restrict__ elems,
+                                   const int* __restrict__ pi, const int* __restrict__ pj, int npairs,
+                                   double* __restrict__ slv, double* __restrict__ dle)
+{
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const int i = pi[p], j = pj[p];
+  const int fi[3] = {elems[3 * i], elems[3 * i + 1], elems[3 * i + 2]};
+  const int fj[3] = {elems[3 * j], elems[3 * j + 1], elems[3 * j + 2]};
+  d3 Pi[3], Pj[3];
+  for (int k = 0; k < 3; k++) {
+    Pi[k] = mk3(nodes[3 * fi[k]], nodes[3 * fi[k] + 1], nodes[3 * fi[k] + 2]);
+    Pj[k] = mk3(nodes[3 * fj[k]], nodes[3 * fj[k] + 1], nodes[3 * fj[k] + 2]);
+  }
+  const PairGeom g = classify_pair(fi, fj, i == j);
+  double s, K[3];
+  near_pair_values(q, g, Pi, Pj, &s, K);
+  slv[p] = s;
+  dle[3 * p] = K[0];
+  dle[3 * p + 1] = K[1];
+  dle[3 * p + 2] = K[2];
+}
+
+__global__ void dl_gather_kernel(const int* __restrict__ cptr, const int* __restrict__ contrib,
+                                 const double* __restrict__ dle, int nslots, double* __restrict__ out)
+{
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  double acc = 0.0;
+  for (int k = cptr[s]; k < cptr[s + 1]; k++) acc += dle[contrib[k]];
+  out[s] = acc;
+}
+
+// ---------------------------------------------------------------------------
+
+static int build_static(Mesh* m)
+{
+  HostMesh& h = m->h;
+  const int ne = h.ne, Q = h.Q, K = h.K;
+  std::vector<float4> pos32((size_t)ne * Q), tgt32((size_t)h.nitems * K);
+  std::vector<dq> pos64((size_t)ne * Q), trin(ne), tgt64((size_t)h.nitems * K), tcent(h.nitems), ccent(h.ncells);
+  std::vector<int4> svid(ne), tvid(h.nitems);
+  std::vector<double> bary(2 * (size_t)Q);
+  for (int b = 0; b < Q; b++) {
+    bary[2 * b] = h.quad.tx[b];
+    bary[2 * b + 1] = h.quad.ty[b];
+  }
+  for (int c = 0; c < h.ncells; c++)
+    ccent[c] = dq{h.cell_center[3 * c], h.cell_center[3 * c + 1], h.cell_center[3 * c + 2], 0.0};
+  for (int s = 0; s < ne; s++) {
+    const int i = h.perm[s];
+    const int* f = &h.elems[3 * i];
+    d3 P[3];
+    for (int k = 0; k < 3; k++) P[k] = mk3(h.nodes[3 * f[k]], h.nodes[3 * f[k] + 1], h.nodes[3 * f[k] + 2]);
+    const d3 w = P[1] - P[0], z = P[2] - P[0];
+    const d3 n = cross3(w, z);
+    const double J = std::sqrt(dot3(n, n));
+    trin[s] = dq{n.x / J, n.y / J, n.z / J, J};
+    svid[s] = make_int4(f[0], f[1], f[2], 0);
+    const int cell = s / kCell;
+    const d3 cc = mk3(h.cell_center[3 * cell], h.cell_center[3 * cell + 1], h.cell_center[3 * cell + 2]);
+    for (int b = 0; b < Q; b++) {
+      const d3 y = P[0] + h.quad.tx[b] * w + h.quad.ty[b] * z;
+      const double wj = h.quad.tw[b] * J;
+      pos64[(size_t)s * Q + b] = dq{y.x, y.y, y.z, wj};
+      const d3 yr = y - cc;
+      pos32[(size_t)s * Q + b] = make_float4((float)yr.x, (float)yr.y, (float)yr.z, (float)wj);
+    }
+    const d3 cen = (1.0 / 3.0) * (P[0] + P[1] + P[2]);
+    for (int ch = 0; ch < h.nchunk; ch++) {
+      const int item = s * h.nchunk + ch;
+      tcent[item] = dq{cen.x, cen.y, cen.z, 0.0};
+      tvid[item] = svid[s];
+      for (int a = 0; a < K; a++) {
+        const int pa = ch * K + a;
+        const int pp = std::min(pa, Q - 1);
+        const double wa = pa < Q ? h.quad.tw[pp] : 0.0;
+        const d3 x = P[0] + h.quad.tx[pp] * w + h.quad.ty[pp] * z;
+        tgt64[(size_t)item * K + a] = dq{x.x, x.y, x.z, wa};
+        const d3 xr = x - cen;
+        tgt32[(size_t)item * K + a] = make_float4((float)xr.x, (float)xr.y, (float)xr.z, (float)wa);
+      }
+    }
+  }
+  EB_CHECK(upload(m->pos32, pos32));
+  EB_CHECK(upload(m->pos64, pos64));
+  EB_CHECK(upload(m->trin, trin));
+  EB_CHECK(upload(m->svid, svid));
+  EB_CHECK(upload(m->perm, h.perm));
+  EB_CHECK(upload(m->iperm, h.iperm));
+  EB_CHECK(upload(m->bary, bary));
+  EB_CHECK(upload(m->tgt32, tgt32));
+  EB_CHECK(upload(m->tgt64, tgt64));
+  EB_CHECK(upload(m->tcent, tcent));
+  EB_CHECK(upload(m->tvid, tvid));
+  EB_CHECK(upload(m->ccent, ccent));
+  return EB_OK;
+}
+
+static int build_near(Mesh* m)
+{
+  HostMesh& h = m->h;
+  const int npairs = (int)h.sl_col.size();
+  m->npairs = npairs;
+  DevBuf d_nodes, d_elems, d_pi, d_pj, d_dle, d_cptr, d_contrib;
+  EB_CHECK(upload(d_nodes, h.nodes));
+  EB_CHECK(upload(d_elems, h.elems));
+  EB_CHECK(upload(d_pi, h.pair_i));
+  EB_CHECK(upload(d_pj, h.sl_col));
+  EB_CHECK(upload(m->sl_rowptr, h.sl_rowptr));
+  EB_CHECK(upload(m->sl_col, h.sl_col));
+  EB_CHECK(upload(m->dl_rowptr, h.dl_rowptr));
+  EB_CHECK(upload(m->dl_col, h.dl_col));
+  EB_CHECK(upload(d_cptr, h.dl_contrib_ptr));
+  EB_CHECK(upload(d_contrib, h.dl_contrib));
+  EB_CHECK(m->sl_val.alloc(sizeof(double) * std::max(npairs, 1)));
+  EB_CHECK(d_dle.alloc(sizeof(double) * 3 * std::max(npairs, 1)));
+  const int nslots = (int)h.dl_col.size();
+  EB_CHECK(m->dl_val.alloc(sizeof(double) * std::max(nslots, 1)));
+  if (npairs > 0) {
+    near_values_kernel<<<(npairs + 127) / 128, 128>>>(h.quad, d_nodes.as<double>(), d_elems.as<int>(),
+                                                      d_pi.as<int>(), d_pj.as<int>(), npairs,
+                                                      m->sl_val.as<double>(), d_dle.as<double>());
+    EB_CUDA(cudaGetLastError());
+  }
+  if (nslots > 0) {
+    dl_gather_kernel<<<(nslots + 255) / 256, 256>>>(d_cptr.as<int>(), d_contrib.as<int>(), d_dle.as<double>(),
+                                                   nslots, m->dl_val.as<double>());
+    EB_CUDA(cudaGetLastError());
+  }
+  EB_CUDA(cudaDeviceSynchronize());
+  return EB_OK;
+}
+
+static size_t slot_bytes(bool fp32) { return fp32 ? sizeof(float4) : sizeof(dq); }
+
+// Source triangles per shared-memory tile for a variant (whole cells when
+// they fit; large quadrature rules fall back to smaller tiles).
+static int src_tile_for(int Q, bool fp32, int nsl, bool dl)
+{
+  const size_t per_tri = (size_t)Q * rec_slots(nsl, dl) * slot_bytes(fp32);
+  const size_t budget = 40 * 1024;
+  int ts = (int)std::min<size_t>(kTS, budget / per_tri);
+  return std::max(ts, 1);
+}
+
+static int build_items(Mesh* m)
+{
+  HostMesh& h = m->h;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+  const int ntt = (h.nitems + kTT - 1) / kTT;
+  const int want = nsm * 32;  // work items for balance across persistent CTAs
+  int nsplit = std::max(1, std::min(h.ncells, (want + ntt - 1) / ntt));
+  const int cells_per = (h.ncells + nsplit - 1) / nsplit;
+  nsplit = (h.ncells + cells_per - 1) / cells_per;
+  std::vector<WorkItem> items;
+  items.reserve((size_t)ntt * nsplit);
+  for (int sp = 0; sp < nsplit; sp++)
+    for (int t = 0; t < ntt; t++)
+      items.push_back(WorkItem{0, t * kTT, sp * cells_per, std::min(h.ncells, (sp + 1) * cells_per), sp});
+  m->plan.nsplit = nsplit;
+  m->nitems_work = (int)items.size();
+  EB_CHECK(upload(m->items, items));
+  EB_CHECK(m->counter.alloc(sizeof(int)));
+  return EB_OK;
+}
+
+int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int order, Mesh** out)
+{
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return set_error(EB_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  Mesh* m = new Mesh();
+  cudaGetDevice(&m->device);
+  int st = prepare_host_mesh(nv, nodes, ne, elems1, order, &m->h);
+  if (st == EB_OK) st = build_static(m);
+  if (st == EB_OK) st = build_near(m);
+  if (st == EB_OK) st = build_items(m);
+  if (st != EB_OK) {
+    delete m;
+    return st;
+  }
+  *out = m;
+  return EB_OK;
+}
+
+int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
+               double* d_q, cudaStream_t st)
+{
+  HostMesh& h = m->h;
+  const bool fp32 = precision == EB_PREC_MIXED;
+  if (precision != EB_PREC_MIXED && precision != EB_PREC_FP64)
+    return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
+  if (!far_variant_supported(nsl, dl)) return set_error(EB_ERR_INVALID, "unsupported operator combination");
+  if ((nsl > 0 && (!d_t || !d_v)) || (dl && (!d_u || !d_q))) return set_error(EB_ERR_INVALID, "null vector");
+  const int nrec = rec_slots(nsl, dl);
+  const size_t sb = slot_bytes(fp32);
+  // Scratch sized once for the largest variant, so device pointers captured
+  // in descriptors (and in CUDA graphs) stay valid.
+  if (!m->rec.p) {
+    EB_CHECK(m->rec.alloc((size_t)h.ne * h.Q * kMaxRecSlots * sizeof(dq)));
+    EB_CHECK(m->partial.alloc(sizeof(double) * (size_t)kMaxOutputs * m->plan.nsplit * h.nitems));
+  }
+  Mesh::Variant& var = m->variants[(fp32 ? 64 : 0) + nsl * 2 + (dl ? 1 : 0)];
+  if (!var.desc.p) {
+    FarMeshDesc desc;
+    desc.tgt32 = m->tgt32.as<float4>();
+    desc.tgt64 = m->tgt64.as<dq>();
+    desc.tcent = m->tcent.as<dq>();
+    desc.tvid = m->tvid.as<int4>();
+    desc.rec = m->rec.p;
+    desc.svid = m->svid.as<int4>();
+    desc.ccent = m->ccent.as<dq>();
+    desc.partial = m->partial.as<double>();
+    desc.nitems = h.nitems;
+    desc.ne = h.ne;
+    desc.Q = h.Q;
+    desc.nsplit = m->plan.nsplit;
+    desc.src_tile = src_tile_for(h.Q, fp32, nsl, dl);
+    const size_t smem = (size_t)desc.src_tile * h.Q * nrec * sb;
+    int occ = far_occupancy(fp32, nsl, dl, h.K, h.Q, smem);
+    if (occ < 1) occ = 1;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    EB_CHECK(var.desc.alloc(sizeof(FarMeshDesc)));
+    EB_CUDA(cudaMemcpy(var.desc.p, &desc, sizeof desc, cudaMemcpyHostToDevice));
+    var.grid = std::min(nsm * occ, std::max(1, m->nitems_work));
+    var.smem = smem;
+    var.src_tile = desc.src_tile;
+  }
+  const void* pos = fp32 ? m->pos32.p : m->pos64.p;
+  EB_CUDA(prep_launch(fp32, nsl, dl, h.ne, h.Q, pos, m->trin.as<dq>(), m->svid.as<int4>(), m->perm.as<int>(),
+                      m->bary.as<double>(), d_t, h.ne, d_u, m->rec.p, st));
+  EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
+  if (m->profile) {
+    if (!m->ev0) {
+      EB_CUDA(cudaEventCreate(&m->ev0));
+      EB_CUDA(cudaEventCreate(&m->ev1));
+      EB_CUDA(cudaEventCreate(&m->ev2));
+    }
+    EB_CUDA(cudaEventRecord(m->ev0, st));
+  }
+  EB_CUDA(far_launch(fp32, nsl, dl, h.K, h.Q, var.desc.as<FarMeshDesc>(), m->items.as<WorkItem>(), m->nitems_work,
+                     m->counter.as<int>(), var.smem, var.grid, st));
+  m->plan.grid = var.grid;
+  m->plan.smem = var.smem;
+  m->plan.src_tile = var.src_tile;
+  if (m->profile) EB_CUDA(cudaEventRecord(m->ev1, st));
+  EB_CUDA(finalize_launch(nsl, dl, h.ne, h.nchunk, m->plan.nsplit, h.nitems, m->iperm.as<int>(), m->trin.as<dq>(),
+                          m->partial.as<double>(), m->sl_rowptr.as<int>(), m->sl_col.as<int>(),
+                          m->sl_val.as<double>(), m->dl_rowptr.as<int>(), m->dl_col.as<int>(),
+                          m->dl_val.as<double>(), d_t, h.ne, d_u, d_v, h.ne, d_q, st));
+  if (m->profile) EB_CUDA(cudaEventRecord(m->ev2, st));
+  return EB_OK;
+}
+
+}  // namespace eb
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+struct eb_mesh_s {
+  eb::Mesh* m = nullptr;
+  cudaStream_t stream = nullptr;
+  std::mutex lock;  // serialises host-buffer calls on one handle
+};
+
+using eb::set_error;
+
+extern "C" {
+
+const char* eb_version(void) { return "easybem-b200 0.1"; }
+const char* eb_last_error(void) { return eb::last_error(); }
+
+int eb_mesh_create(int nnodes, const double* nodes, int nelems, const int* elems, int order, eb_mesh* out)
+{
+  if (!out) return set_error(EB_ERR_INVALID, "null output handle");
+  *out = nullptr;
+  eb::Mesh* m = nullptr;
+  int st = eb::mesh_create(nnodes, nodes, nelems, elems, order, &m);
+  if (st != EB_OK) return st;
+  eb_mesh h = new eb_mesh_s();
+  h->m = m;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete m;
+    delete h;
+    return set_error(EB_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return EB_OK;
+}
+
+int eb_mesh_destroy(eb_mesh mesh)
+{
+  if (!mesh) return EB_OK;
+  cudaSetDevice(mesh->m->device);
+  if (mesh->stream) {
+    cudaStreamSynchronize(mesh->stream);
+    cudaStreamDestroy(mesh->stream);
+  }
+  delete mesh->m;
+  delete mesh;
+  return EB_OK;
+}
+
+int eb_mesh_info(eb_mesh mesh, int* nnodes, int* nelems, long long* near_pairs, long long* far_quad_pairs)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  if (nnodes) *nnodes = mesh->m->h.nv;
+  if (nelems) *nelems = mesh->m->h.ne;
+  if (near_pairs) *near_pairs = mesh->m->npairs;
+  if (far_quad_pairs) *far_quad_pairs = mesh->m->h.far_quad_pairs;
+  return EB_OK;
+}
+
+int eb_apply_sl_dl_device(eb_mesh mesh, int precision, const double* d_t, const double* d_u, double* d_v,
+                          double* d_q, void* stream)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  const bool sl = d_t && d_v;
+  const bool dl = d_u && d_q;
+  if (!sl && !dl) return set_error(EB_ERR_INVALID, "nothing to apply: pass t/v and/or u/q");
+  EB_CUDA(cudaSetDevice(mesh->m->device));
+  return eb::mesh_apply(mesh->m, precision, sl ? 1 : 0, dl, d_t, d_u, d_v, d_q, (cudaStream_t)stream);
+}
+
+static int host_apply(eb_mesh mesh, int precision, const double* t, const double* u, double* v, double* q)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  std::lock_guard<std::mutex> g(mesh->lock);
+  eb::Mesh* m = mesh->m;
+  EB_CUDA(cudaSetDevice(m->device));
+  const int ne = m->h.ne, nv = m->h.nv;
+  const bool sl = t && v, dl = u && q;
+  cudaStream_t st = mesh->stream;
+  if (sl) {
+    EB_CHECK(m->io_t.alloc(sizeof(double) * ne));
+    EB_CHECK(m->io_v.alloc(sizeof(double) * ne));
+    EB_CUDA(cudaMemcpyAsync(m->io_t.p, t, sizeof(double) * ne, cudaMemcpyHostToDevice, st));
+  }
+  if (dl) {
+    EB_CHECK(m->io_u.alloc(sizeof(double) * nv));
+    EB_CHECK(m->io_q.alloc(sizeof(double) * ne));
+    EB_CUDA(cudaMemcpyAsync(m->io_u.p, u, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+  }
+  EB_CHECK(eb::mesh_apply(m, precision, sl ? 1 : 0, dl, sl ? m->io_t.as<double>() : nullptr,
+                          dl ? m->io_u.as<double>() : nullptr, sl ? m->io_v.as<double>() : nullptr,
+                          dl ? m->io_q.as<double>() : nullptr, st));
+  if (sl) EB_CUDA(cudaMemcpyAsync(v, m->io_v.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
+  if (dl) EB_CUDA(cudaMemcpyAsync(q, m->io_q.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
+  EB_CUDA(cudaStreamSynchronize(st));
+  return EB_OK;
+}
+
+int eb_apply_sl_p0(eb_mesh mesh, int precision, const double* t, double* v)
+{
+  if (!t || !v) return set_error(EB_ERR_INVALID, "null vector");
+  return host_apply(mesh, precision, t, nullptr, v, nullptr);
+}
+
+int eb_apply_dl_p1(eb_mesh mesh, int precision, const double* u, double* q)
+{
+  if (!u || !q) return set_error(EB_ERR_INVALID, "null vector");
+  return host_apply(mesh, precision, nullptr, u, nullptr, q);
+}
+
+int eb_apply_sl_dl(eb_mesh mesh, int precision, const double* t, const double* u, double* v, double* q)
+{
+  if (!t || !u || !v || !q) return set_error(EB_ERR_INVALID, "null vector");
+  return host_apply(mesh, precision, t, u, v, q);
+}
+
+int eb_quadrature(int order, int* nline, double* lx, double* lw, int* ntri, double* tx, double* ty, double* tw)
+{
+  eb::Quadrature q;
+  if (!eb::make_quadrature(order, &q))
+    return set_error(EB_ERR_INVALID, "quadrature order must be in 0.." + std::to_string(eb::kMaxOrder));
+  if (nline) *nline = q.nl;
+  if (ntri) *ntri = q.nt;
+  for (int i = 0; i < q.nl; i++) {
+    if (lx) lx[i] = q.lx[i];
+    if (lw) lw[i] = q.lw[i];
+  }
+  for (int i = 0; i < q.nt; i++) {
+    if (tx) tx[i] = q.tx[i];
+    if (ty) ty[i] = q.ty[i];
+    if (tw) tw[i] = q.tw[i];
+  }
+  return EB_OK;
+}
+
+int eb_set_profiling(eb_mesh mesh, int on)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  mesh->m->profile = on != 0;
+  return EB_OK;
+}
+
+int eb_last_kernel_ms(eb_mesh mesh, double* far_ms, double* finalize_ms)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  eb::Mesh* m = mesh->m;
+  if (!m->profile || !m->ev0) return set_error(EB_ERR_STATE, "profiling is off or nothing was applied");
+  EB_CUDA(cudaEventSynchronize(m->ev2));
+  float a = 0.f, b = 0.f;
+  EB_CUDA(cudaEventElapsedTime(&a, m->ev0, m->ev1));
+  EB_CUDA(cudaEventElapsedTime(&b, m->ev1, m->ev2));
+  if (far_ms) *far_ms = a;
+  if (finalize_ms) *finalize_ms = b;
+  return EB_OK;
+}
+
+int eb_apply_sl_p1(eb_mesh mesh, int precision, const double* t, double* v)
+{
+  (void)mesh; (void)precision; (void)t; (void)v;
+  return set_error(EB_ERR_STATE, "eb_apply_sl_p1 is not available in this build yet");
+}
+
+int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double* q)
+{
+  (void)mesh; (void)precision; (void)u; (void)q;
+  return set_error(EB_ERR_STATE, "eb_apply_hypersingular is not available in this build yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// Device-resident mesh and the apply pipeline.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "farfield.cuh"
+#include "mesh_host.h"
+
+namespace eb {
+
+cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
+                       int* dc, size_t smem, int grid, cudaStream_t st);
+int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem);
+bool far_variant_supported(int NSL, bool DL);
+cudaError_t prep_launch(bool fp32, int NSL, bool DL, int ne, int Q, const void* pos, const dq* trin, const int4* svid,
+                        const int* perm, const double* bary, const double* t, int tstride, const double* u, void* rec,
+                        cudaStream_t st);
+cudaError_t finalize_launch(int NSL, bool DL, int ne, int nchunk, int nsplit, int nitems, const int* iperm,
+                            const dq* trin, const double* partial, const int* sl_rowptr, const int* sl_col,
+                            const double* sl_val, const int* dl_rowptr, const int* dl_col, const double* dl_val,
+                            const double* t, int tstride, const double* u, double* v, int vstride, double* q,
+                            cudaStream_t st);
+
+// Simple owning device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { release(); }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  int alloc(size_t n);  // no-op when already at least n bytes
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// Launch plan of the far field for one mesh (tile shape and work split).
+struct FarPlan {
+  int src_tile = kTS;  // source triangles per shared-memory tile
+  int nsplit = 1;      // source ranges per target tile
+  int grid = 0;        // persistent CTAs
+  size_t smem = 0;
+};
+
+struct Mesh {
+  HostMesh h;
+  int device = 0;
+
+  // static geometry (sorted order)
+  DevBuf pos32, pos64, trin, svid, perm, iperm, bary;
+  DevBuf tgt32, tgt64, tcent, tvid, ccent;
+  // near field
+  DevBuf sl_rowptr, sl_col, sl_val, dl_rowptr, dl_col, dl_val;
+  long long npairs = 0;
+  // per-apply scratch
+  DevBuf rec, partial, counter, items;
+  DevBuf io_t, io_u, io_v, io_q;
+  int nitems_work = 0;
+  FarPlan plan;
+  // one immutable device descriptor and launch shape per far-field variant
+  // (key = fp32 * 64 + nsl * 2 + dl), so a queued launch never sees it change
+  struct Variant {
+    DevBuf desc;
+    int grid = 0;
+    size_t smem = 0;
+    int src_tile = 0;
+  };
+  Variant variants[128];
+  // optional event timing of the far-field kernel
+  bool profile = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  float last_far_ms = 0.f, last_fin_ms = 0.f;
+
+  ~Mesh();
+};
+
+int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int order, Mesh** out);
+// Device-pointer apply: t has nsl columns (stride ne), v likewise; u/q for DL.
+int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
+               double* d_q, cudaStream_t st);
+
+}  // namespace eb

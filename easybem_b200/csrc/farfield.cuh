@@ -1,0 +1,76 @@
+// Far-field kernels: the regular triangle-pair Gauss quadrature treated as an
+// N-body sum over quadrature points.
+//
+// The reference evaluates one triangle pair per thread from host-packed
+// geometry (src/BEM3dLaplaceGPU.cu:445-488 SL, :775-827 DL, launched from
+// :1292 and :1533). Here each thread owns the quadrature points of one target
+// triangle (item), a CTA owns kTT targets, and source quadrature points are
+// staged through shared memory in tiles and broadcast to all threads:
+//
+//   SL:  acc_a += c_b / |x_a - y_b|,          c_b = w_b J_j t_j
+//   DL:  acc_a += (x_a - y_b).p_b / |x_a-y_b|^3, p_b = w_b J_j u_h(y_b) n_j
+//
+// with the target weights w_a J_i / (4 pi) applied when the item is folded.
+// Pairs of triangles sharing a vertex are skipped (the FP64 Sauter-Schwab
+// near field supplies them). Each work item covers one target tile and one
+// contiguous range of source cells; results of different items go to
+// separate partial slots, summed in a fixed order by the finalize kernel, so
+// the result is bitwise reproducible regardless of scheduling.
+//
+// FP32 variant: coordinates are stored relative to the centre of the source
+// cell (kCell triangles) and of the target triangle, the per-cell offset is
+// formed in FP64, so |x - y| keeps full FP32 relative accuracy for close
+// pairs; per-cell partial sums are folded into a two-sum (float-float)
+// accumulator per target item.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.h"
+
+namespace eb {
+
+constexpr int kTT = 128;  // target items (threads) per CTA
+constexpr int kTS = 64;   // source triangles per shared-memory tile (Q <= 7)
+constexpr int kMaxRecSlots = 3;  // record slots of the widest variant
+constexpr int kMaxOutputs = 5;   // SL charges + DL of the widest variant
+
+// FP64 record slot (two 16-byte halves).
+struct __align__(16) dq {
+  double x, y, z, w;
+};
+
+// Number of 16/32-byte record slots per source point.
+__host__ __device__ constexpr int rec_slots(int nsl, bool dl)
+{
+  return 1 + (dl ? 1 : 0) + ((nsl - (dl ? 2 : 1)) > 0 ? ((nsl - (dl ? 2 : 1)) + 3) / 4 : 0);
+}
+
+// Slot and component of charge r in a record.
+__host__ __device__ inline void charge_slot(int r, bool dl, int* slot, int* comp)
+{
+  if (r == 0) { *slot = 0; *comp = 3; return; }
+  if (r == 1 && dl) { *slot = 1; *comp = 3; return; }
+  const int k = r - (dl ? 2 : 1);
+  *slot = (dl ? 2 : 1) + k / 4;
+  *comp = k % 4;
+}
+
+// Per-mesh view used by the far-field kernels (device pointers).
+struct FarMeshDesc {
+  const float4* tgt32;  // [nitems*K]: (x_a - centroid) in FP32, weight w_a
+  const dq* tgt64;      // [nitems*K]: x_a in FP64, weight w_a
+  const dq* tcent;      // [nitems]: centroid of the item's triangle (FP64)
+  const int4* tvid;     // [nitems]: vertex ids of the item's triangle (-1 if padding)
+  const void* rec;      // [ne*Q*nrec] source records (float4 or dq), sorted order
+  const int4* svid;     // [ne]: vertex ids of sorted source triangles
+  const dq* ccent;      // [ncells]: cell centres (FP64)
+  double* partial;      // [nout][nsplit][nitems]
+  int nitems, ne, Q, nsplit, src_tile;
+};
+
+struct WorkItem {
+  int mesh, tgt0, cell0, cell1, split;
+};
+
+}  // namespace eb

@@ -1,0 +1,99 @@
+/*
+ * easybem B200 — C ABI of the matrix-free Galerkin layer-potential apply.
+ *
+ * Plain pointers and sizes only. Every entry point returns an int status
+ * (EB_OK on success); eb_last_error() returns a message for the last failure
+ * on the calling thread. Elements are 1-based vertex triples, as in easybem.
+ *
+ * The reference exposes this path as process-global C++ functions
+ * (include/BEM3dLaplaceGPU.h:8-18) bound to Python in python/bindings.cpp:
+ * 186-253. This ABI is the handle-based form of the same operations; the
+ * legacy C++ symbols (include/BEM3dLaplaceGPU.h of this project) are a thin
+ * shim over one default handle.
+ */
+#ifndef EASYBEM_GPU_H
+#define EASYBEM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EB_OK 0
+#define EB_ERR_INVALID 1        /* bad argument: null pointer, size, order index */
+#define EB_ERR_MESH 2           /* vertex index out of range, repeated or degenerate triangle */
+#define EB_ERR_CUDA 3           /* a CUDA runtime call failed */
+#define EB_ERR_NOMEM 4          /* device memory exhausted or over a budget */
+#define EB_ERR_TIMEOUT 5        /* a bounded device-side wait ran out */
+#define EB_ERR_STATE 6          /* call out of order (no mesh, closed server) */
+#define EB_ERR_NOT_CONVERGED 7  /* a solve stopped at its iteration limit */
+
+/* Far-field arithmetic. The Sauter-Schwab near field is always FP64. */
+#define EB_PREC_FP64 0  /* plain FP64: the default */
+#define EB_PREC_MIXED 1 /* FP32 far field with compensated (two-sum) row sums */
+
+typedef struct eb_mesh_s* eb_mesh;
+
+const char* eb_version(void);
+const char* eb_last_error(void);
+
+/* Uploads a closed or open triangulated surface and precomputes, once, the
+ * FP64 Sauter-Schwab near-field correction (coincident, edge- and
+ * vertex-adjacent pairs) and the far-field quadrature points. `order` is the
+ * easybem quadrature index (0..18, default 4). Replaces initGPU
+ * (src/BEM3dLaplaceGPU.cu:830-921 with src/meshTopology.cpp:196-261). */
+int eb_mesh_create(int nnodes, const double* nodes, int nelems, const int* elems, int order,
+                   eb_mesh* out);
+/* Releases a mesh. Replaces closeGPU (src/BEM3dLaplaceGPU.cu:924-957). */
+int eb_mesh_destroy(eb_mesh mesh);
+/* Sizes: vertices, triangles, near pairs (incl. coincident) and the number of
+ * regular quadrature-point pairs one far-field apply evaluates. */
+int eb_mesh_info(eb_mesh mesh, int* nnodes, int* nelems, long long* near_pairs,
+                 long long* far_quad_pairs);
+
+/* v = V t, the P0 single layer (Galerkin, kernel 1/(4 pi |x-y|)); t and v
+ * have nelems entries, host memory. Replaces applyGPULaplace3d1Layer(t, v, 0)
+ * (src/BEM3dLaplaceGPU.cu:985-1322). */
+int eb_apply_sl_p0(eb_mesh mesh, int precision, const double* t, double* v);
+/* q = K u, the double layer with P0 test and P1 trial functions; u has
+ * nnodes entries, q nelems, host memory. Replaces applyGPULaplace3d2Layer
+ * (src/BEM3dLaplaceGPU.cu:1325-1551). */
+int eb_apply_dl_p1(eb_mesh mesh, int precision, const double* u, double* q);
+/* Both applies in one pass over the pairs (shared distance evaluation). */
+int eb_apply_sl_dl(eb_mesh mesh, int precision, const double* t, const double* u, double* v,
+                   double* q);
+/* Device-pointer form on a CUDA stream (cudaStream_t passed as void*; null
+ * selects the legacy default stream). Any of t/v or u/q may be null to skip
+ * that operator. Asynchronous: the caller synchronises the stream. */
+int eb_apply_sl_dl_device(eb_mesh mesh, int precision, const double* d_t, const double* d_u,
+                          double* d_v, double* d_q, void* stream);
+
+/* v = V1 t, the single layer with P1 test and trial functions (t, v have
+ * nnodes entries). Replaces applyGPULaplace3d1Layer(t, v, 1)
+ * (src/BEM3dLaplaceGPU.cu:82-154, 211-320, 371-442, 491-557, host :1034-1313). */
+int eb_apply_sl_p1(eb_mesh mesh, int precision, const double* t, double* v);
+/* q = D u, the hypersingular operator in the curl form
+ * D = sum_k C_k^T V C_k of getLaplace3d (src/BEM3dLaplace.cpp:767-771); u, q
+ * have nnodes entries. Replaces the empty applyGPULaplace3dHyperSing
+ * (src/BEM3dLaplaceGPU.cu:1554-1555). */
+int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double* q);
+
+/* The quadrature rules behind index `order` (host only, no GPU needed):
+ * the Gauss-Legendre rule on [0,1] (up to 64 points) and the triangle rule on
+ * the reference triangle (up to 79 points, weights summing to 1/2). Mirrors
+ * the tables LineQuadrature* / TriangleQuadrature* of src/quadrature.cpp:
+ * 284-305, 1045-1070. Arrays must hold 64 and 79 entries. */
+int eb_quadrature(int order, int* nline, double* lx, double* lw, int* ntri, double* tx, double* ty,
+                  double* tw);
+
+/* Event timing of the far-field kernel and of the finalize kernel (which
+ * includes the near-field SpMV) of the last apply on this mesh, recorded on
+ * the apply's stream when profiling is on. Blocks until that apply ends.
+ * No counterpart in the reference (which has no timing API). */
+int eb_set_profiling(eb_mesh mesh, int on);
+int eb_last_kernel_ms(eb_mesh mesh, double* far_ms, double* finalize_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EASYBEM_GPU_H */

@@ -1,0 +1,137 @@
+"""GPU parity of the matrix-free SL (P0) and DL (P0 x P1) applies.
+
+The CUDA path (through the C ABI) against the reference's FP64 operators:
+committed golden outputs of the reference's own CPU code for small meshes at
+several quadrature indices, and the pinned CPU oracle on sampled rows of
+large meshes. Tolerances (relative L2):
+  plain FP64 apply            <= 1e-12
+  mixed (FP32 far field)      <= 1e-6
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from easybem_b200 import meshes
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-6
+
+
+@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16"])
+def test_small_meshes_match_reference_golden(gpu_lib, golden_ops, name):
+    z = golden_ops
+    nodes, elems, t, u = z[f"{name}_nodes"], z[f"{name}_elems"], z[f"{name}_t"], z[f"{name}_u"]
+    with gpu_lib.Mesh(nodes, elems, 4) as m:
+        v, q = m.apply_sl_dl(t, u)
+        assert rel_l2(v, z[f"{name}_o4_Vt"]) < FP64_TOL
+        assert rel_l2(q, z[f"{name}_o4_Ku"]) < FP64_TOL
+        v32, q32 = m.apply_sl_dl(t, u, precision="mixed")
+        assert rel_l2(v32, z[f"{name}_o4_Vt"]) < MIXED_TOL
+        assert rel_l2(q32, z[f"{name}_o4_Ku"]) < MIXED_TOL
+
+
+def test_quadrature_orders_match_reference_golden(gpu_lib, golden_ops):
+    z = golden_ops
+    nodes, elems, t, u = z["pico2_nodes"], z["pico2_elems"], z["pico2_t"], z["pico2_u"]
+    for o in z["pico2_orders"]:
+        with gpu_lib.Mesh(nodes, elems, int(o)) as m:
+            v, q = m.apply_sl_dl(t, u)
+            assert rel_l2(v, z[f"pico2_o{o}_Vt"]) < FP64_TOL, o
+            assert rel_l2(q, z[f"pico2_o{o}_Ku"]) < FP64_TOL, o
+            v32, q32 = m.apply_sl_dl(t, u, precision="mixed")
+            assert rel_l2(v32, z[f"pico2_o{o}_Vt"]) < MIXED_TOL, o
+            assert rel_l2(q32, z[f"pico2_o{o}_Ku"]) < MIXED_TOL, o
+
+
+def test_separate_and_fused_applies_agree(gpu_lib, golden_ops):
+    z = golden_ops
+    nodes, elems, t, u = z["pico2_nodes"], z["pico2_elems"], z["pico2_t"], z["pico2_u"]
+    with gpu_lib.Mesh(nodes, elems) as m:
+        v, q = m.apply_sl_dl(t, u)
+        assert rel_l2(m.apply_sl(t), v) < 1e-14
+        assert rel_l2(m.apply_dl(u), q) < 1e-14
+
+
+@pytest.mark.parametrize("level,nrows", [(4, 128), (6, 24)])
+def test_large_mesh_sampled_rows_vs_oracle(gpu_lib, oracle, level, nrows):
+    nodes, elems = meshes.perturbed_icosphere(level, seed=1)
+    rng = np.random.default_rng(level)
+    t = rng.normal(size=elems.shape[0])
+    u = rng.normal(size=nodes.shape[0])
+    rows = np.sort(rng.choice(elems.shape[0], nrows, replace=False)).astype(np.int32)
+    oracle.set_order(4)
+    vo, qo = oracle.apply_rows(nodes, elems, t, u, rows)
+    with gpu_lib.Mesh(nodes, elems) as m:
+        v, q = m.apply_sl_dl(t, u)
+        assert rel_l2(v[rows], vo) < FP64_TOL
+        assert rel_l2(q[rows], qo) < FP64_TOL
+        v32, q32 = m.apply_sl_dl(t, u, precision="mixed")
+        assert rel_l2(v32[rows], vo) < MIXED_TOL
+        assert rel_l2(q32[rows], qo) < MIXED_TOL
+        # full-vector agreement of the two precisions (a size-independent check)
+        assert rel_l2(v32, v) < MIXED_TOL
+        assert rel_l2(q32, q) < MIXED_TOL
+
+
+def test_applies_are_bitwise_reproducible(gpu_lib):
+    nodes, elems = meshes.perturbed_icosphere(4, seed=2)
+    rng = np.random.default_rng(0)
+    t = rng.normal(size=elems.shape[0])
+    u = rng.normal(size=nodes.shape[0])
+    with gpu_lib.Mesh(nodes, elems) as m:
+        for prec in ("fp64", "mixed"):
+            a = m.apply_sl_dl(t, u, precision=prec)
+            b = m.apply_sl_dl(t, u, precision=prec)
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_linearity_and_gauss_identity(gpu_lib):
+    nodes, elems = meshes.perturbed_icosphere(5, seed=3)
+    rng = np.random.default_rng(1)
+    t1, t2 = rng.normal(size=(2, elems.shape[0]))
+    with gpu_lib.Mesh(nodes, elems) as m:
+        v1, v2, v12 = m.apply_sl(t1), m.apply_sl(t2), m.apply_sl(2.0 * t1 - 3.0 * t2)
+        assert rel_l2(v12, 2.0 * v1 - 3.0 * v2) < 1e-13
+        # K 1 = -1/2 M 1 on a closed surface, M 1 = triangle areas
+        q = m.apply_dl(np.ones(nodes.shape[0]))
+        P = nodes[elems - 1]
+        area = 0.5 * np.linalg.norm(np.cross(P[:, 1] - P[:, 0], P[:, 2] - P[:, 0]), axis=1)
+        assert abs(q.sum() / area.sum() + 0.5) < 1e-3
+
+
+def test_legacy_module_api(gpu_lib, golden_ops):
+    z = golden_ops
+    nodes, elems, t, u = z["ico2_nodes"], z["ico2_elems"], z["ico2_t"], z["ico2_u"]
+    gpu_lib.init_gpu(nodes, elems, 4, 240, 32)
+    try:
+        v = gpu_lib.apply_gpu_laplace3d_1layer(t)
+        q = gpu_lib.apply_gpu_laplace3d_2layer(u)
+        assert v.shape == (elems.shape[0],) and q.shape == (elems.shape[0],)
+        assert rel_l2(v, z["ico2_o4_Vt"]) < FP64_TOL
+        assert rel_l2(q, z["ico2_o4_Ku"]) < FP64_TOL
+    finally:
+        gpu_lib.close_gpu()
+
+
+def test_invalid_meshes_are_rejected(gpu_lib):
+    from easybem_b200 import EasyBemError
+    nodes, elems = meshes.icosphere(1)
+    bad = elems.copy()
+    bad[3, 1] = nodes.shape[0] + 1
+    with pytest.raises(EasyBemError) as e:
+        gpu_lib.Mesh(nodes, bad)
+    assert e.value.status == 2
+    bad = elems.copy()
+    bad[0, 1] = bad[0, 0]
+    with pytest.raises(EasyBemError):
+        gpu_lib.Mesh(nodes, bad)
+    flat = nodes.copy()
+    f0 = elems[0] - 1
+    flat[f0[2]] = flat[f0[0]] * 0.5 + flat[f0[1]] * 0.5
+    with pytest.raises(EasyBemError):
+        gpu_lib.Mesh(flat, elems)
+    with pytest.raises(EasyBemError) as e:
+        gpu_lib.Mesh(nodes, elems, order=19)
+    assert e.value.status == 1

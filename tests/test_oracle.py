@@ -1,0 +1,105 @@
+"""The CPU oracle (oracle/bem_oracle.c) pinned against the reference.
+
+Two pins: the committed golden fixtures made from the reference's own CPU
+code (tests/golden/make_golden.py), and — where oracle/_ref was built from
+the reference sources — direct comparisons of every pair routine and of the
+matrix-free apply with the reference functions.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from easybem_b200 import meshes
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16"])
+def test_oracle_matches_golden_default_order(golden_ops, oracle, name):
+    z = golden_ops
+    nodes, elems, t, u = z[f"{name}_nodes"], z[f"{name}_elems"], z[f"{name}_t"], z[f"{name}_u"]
+    oracle.set_order(4)
+    v, q = oracle.apply_rows(nodes, elems, t, u)
+    assert rel_l2(v, z[f"{name}_o4_Vt"]) < 1e-13
+    assert rel_l2(q, z[f"{name}_o4_Ku"]) < 1e-13
+
+
+def test_oracle_matches_golden_all_orders(golden_ops, oracle):
+    z = golden_ops
+    nodes, elems, t, u = z["pico2_nodes"], z["pico2_elems"], z["pico2_t"], z["pico2_u"]
+    for o in z["pico2_orders"]:
+        oracle.set_order(int(o))
+        v, q = oracle.apply_rows(nodes, elems, t, u)
+        assert rel_l2(v, z[f"pico2_o{o}_Vt"]) < 1e-13, o
+        assert rel_l2(q, z[f"pico2_o{o}_Ku"]) < 1e-13, o
+    oracle.set_order(4)
+
+
+def test_oracle_dense_cube_entrywise(golden_ops, oracle):
+    z = golden_ops
+    V, K = oracle.dense(z["cube_nodes"], z["cube_elems"])
+    assert np.max(np.abs(V - z["cube_o4_V"])) < 1e-15
+    assert np.max(np.abs(K - z["cube_o4_K"])) < 1e-15
+
+
+def test_gauss_identity_known_answer(golden_ops, oracle):
+    # K 1 = -1/2 M 1 for the interior limit on a closed surface (up to
+    # discretisation error); measured -0.5000002 on the L3 icosphere.
+    z = golden_ops
+    nodes, elems = z["ico2_nodes"], z["ico2_elems"]
+    _, q = oracle.apply_rows(nodes, elems, None, np.ones(nodes.shape[0]))
+    ratio = q.mean() / z["ico2_M1"].mean()
+    assert abs(ratio + 0.5) < 1e-4
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+def test_pair_routines_match_reference():
+    lib = O.ref_lib()
+    lib.ref_set_order(4)
+    orc = O.Oracle(4)
+    rng = np.random.default_rng(11)
+    for _ in range(20):
+        a, b, c, d, A, B = (rng.normal(size=3) for _ in range(6))
+        P = lambda x: O._d(np.ascontiguousarray(x))
+        assert abs(orc.lib.orc_sl_id(P(a), P(b)) - lib.ref_sl_id(P(a), P(b))) <= 1e-14 * abs(lib.ref_sl_id(P(a), P(b)))
+        r1, r2 = orc.lib.orc_sl_edge(P(a), P(b), P(c)), lib.ref_sl_edge(P(a), P(b), P(c))
+        assert abs(r1 - r2) <= 1e-13 * abs(r2)
+        r1, r2 = orc.lib.orc_sl_vertex(P(a), P(b), P(c), P(d)), lib.ref_sl_vertex(P(a), P(b), P(c), P(d))
+        assert abs(r1 - r2) <= 1e-13 * abs(r2)
+        A2 = A + 5.0
+        r1 = orc.lib.orc_sl_disjoint(P(A2), P(a), P(b), P(B), P(c), P(d))
+        r2 = lib.ref_sl_disjoint(P(A2), P(a), P(b), P(B), P(c), P(d))
+        assert abs(r1 - r2) <= 1e-13 * abs(r2)
+        k1, k2 = np.zeros(3), np.zeros(3)
+        orc.lib.orc_dl_edge(P(a), P(b), P(c), O._d(k1)); lib.ref_dl_edge(P(a), P(b), P(c), O._d(k2))
+        assert np.max(np.abs(k1 - k2)) <= 1e-13 * np.max(np.abs(k2))
+        orc.lib.orc_dl_vertex(P(a), P(b), P(c), P(d), O._d(k1)); lib.ref_dl_vertex(P(a), P(b), P(c), P(d), O._d(k2))
+        assert np.max(np.abs(k1 - k2)) <= 1e-13 * np.max(np.abs(k2))
+        orc.lib.orc_dl_disjoint(P(A2), P(a), P(b), P(B), P(c), P(d), O._d(k1))
+        lib.ref_dl_disjoint(P(A2), P(a), P(b), P(B), P(c), P(d), O._d(k2))
+        assert np.max(np.abs(k1 - k2)) <= 1e-13 * np.max(np.abs(k2))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+def test_matrix_free_apply_matches_reference_sampled_rows():
+    nodes, elems = meshes.perturbed_icosphere(3, seed=5)
+    rng = np.random.default_rng(2)
+    t = rng.normal(size=elems.shape[0])
+    u = rng.normal(size=nodes.shape[0])
+    rows = np.sort(rng.choice(elems.shape[0], 64, replace=False)).astype(np.int32)
+    orc = O.Oracle(4)
+    v1, q1 = orc.apply_rows(nodes, elems, t, u, rows)
+    v2, q2 = O.ref_apply_rows(nodes, elems, t, u, rows)
+    assert rel_l2(v1, v2) < 1e-14
+    assert rel_l2(q1, q2) < 1e-14
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+def test_reference_dense_equals_reference_matrix_free():
+    nodes, elems = meshes.icosphere(2)
+    rng = np.random.default_rng(4)
+    t = rng.normal(size=elems.shape[0])
+    u = rng.normal(size=nodes.shape[0])
+    V, K, _, _ = O.ref_dense(nodes, elems, 4)
+    v, q = O.ref_apply_rows(nodes, elems, t, u)
+    assert rel_l2(V @ t, v) < 1e-14
+    assert rel_l2(K @ u, q) < 1e-14
