@@ -1,0 +1,365 @@
+"""Benchmark: matrix-free Galerkin SL (P0) + DL (P0 x P1) apply on one B200.
+
+Workload: the single-mesh matvec of a radius-perturbed icosphere refined 6
+times (81,920 triangles, 40,962 vertices; r = 1 + 0.1 sum_{l<=4} a_lm Y_lm,
+a_lm ~ N(0, 0.2^2), seed 1), quadrature index 4 (7-point triangle rule),
+densities t ~ N(0,1) per triangle and u ~ N(0,1) per vertex. One step is one
+fused SL+DL apply: v = V t and q = K u (far field + FP64 near field).
+
+Metric: quadrature-pair evaluations per second (Gpairs/s); one pair is one
+(x_a, y_b) kernel evaluation of both operators between triangles that share
+no vertex, 49 per triangle pair at index 4. The headline ``value`` is the
+mixed-precision apply (FP32 far field with compensated row sums, FP64 near
+field) with inputs resident in HBM; the plain FP64 apply is reported beside
+it, with the relative L2 error of both against the CPU oracle on sampled
+rows. ``e2e`` repeats the mixed apply through the host-buffer C ABI
+(eb_apply_sl_dl) with pinned host vectors: H2D of t, u and D2H of v, q in
+every step.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+For N > 1 it runs under torch.distributed.run: every rank applies the same
+operator on its own GPU (replicas, no data-path collective; weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SL+DL Galerkin apply Gpairs/s, mixed vs FP64 at 1e-6 rel err; p99 solve ms"
+LEVEL = 6
+SEED = 1
+ORDER = 4
+WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L6 "
+            "(81,920 triangles, 40,962 vertices), quadrature index 4 (Q=7)")
+FLOPS_PER_PAIR = 20  # SL: 3 sub + 5 (|r|^2) + 1 rsqrt + 2 fma; DL: 5 (r.p) + 2 mul + 2 fma (FMA = 2)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--level", type=int, default=LEVEL)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[4:8]):
+                if flag.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        loaded = [x for x in sm if mx is None or x > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_problem(level):
+    from easybem_b200 import meshes
+    nodes, elems = meshes.perturbed_icosphere(level, seed=SEED)
+    rng = np.random.default_rng(2024)
+    t = rng.normal(size=elems.shape[0])
+    u = rng.normal(size=nodes.shape[0])
+    return nodes, elems, t, u
+
+
+def cpu_reference_sample(nodes, elems, t, u, target_s=15.0, nthreads=0):
+    """The reference's own FP64 pair routines (oracle/_ref) on sampled rows,
+    all host threads; falls back to the oracle port when _ref is absent."""
+    from oracle import oracle as O
+    ne = elems.shape[0]
+    rng = np.random.default_rng(99)
+    kind = "reference" if O.ref_available() else "port"
+    run = (lambda rows: O.ref_apply_rows(nodes, elems, t, u, rows, nthreads=nthreads, order=ORDER)) \
+        if kind == "reference" else (lambda rows: O.Oracle(ORDER).apply_rows(nodes, elems, t, u, rows, nthreads))
+    ncores = nthreads or os.cpu_count()
+    nrows = max(ncores, 8)
+    rows = np.sort(rng.choice(ne, nrows, replace=False)).astype(np.int32)
+    a = time.perf_counter(); run(rows); dt = time.perf_counter() - a
+    nrows = int(min(ne, max(nrows, nrows * target_s / max(dt, 1e-3))))
+    rows = np.sort(rng.choice(ne, nrows, replace=False)).astype(np.int32)
+    a = time.perf_counter(); v, q = run(rows); dt = time.perf_counter() - a
+    pairs = nrows * (ne - 13) * 49  # disjoint triangle pairs per row (~13 near) x Q^2
+    return {"value": pairs / dt / 1e9, "unit": "Gpairs/s", "cores": ncores, "kind": kind,
+            "sample": f"{nrows} of {ne} rows of the same SL+DL apply (FP64, {dt:.1f} s)", "seconds": dt}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    nodes, elems, t, u = make_problem(args.level)
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    ne = elems.shape[0]
+    ncores = os.cpu_count()
+    rng = np.random.default_rng(7)
+    # size one step to a few seconds of work
+    probe = cpu_reference_sample(nodes, elems, t, u, target_s=2.0)
+    rows_per_step = max(ncores, int(probe["value"] * 1e9 * 4.0 / ((ne - 13) * 49)))
+    times = []
+    for k in range(args.warmup + args.steps):
+        rows = np.sort(rng.choice(ne, min(ne, rows_per_step), replace=False)).astype(np.int32)
+        a = time.perf_counter()
+        if kind == "reference":
+            O.ref_apply_rows(nodes, elems, t, u, rows, order=ORDER)
+        else:
+            O.Oracle(ORDER).apply_rows(nodes, elems, t, u, rows)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - a)
+    pairs = len(rows) * (ne - 13) * 49
+    value = pairs * len(times) / sum(times) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "Gpairs/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "sample_rows_per_step": len(rows)},
+            "cpu_baseline": {"value": value, "unit": "Gpairs/s", "cores": ncores, "kind": kind,
+                             "sample": f"{len(rows)} of {ne} rows per step, reference FP64 pair routines "
+                                       f"(src/BEM3dLaplace.cpp:22-437) with OpenMP"},
+            "e2e": {"value": value, "unit": "Gpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import easybem_b200 as eb
+    from easybem_b200 import _lib
+
+    nodes, elems, t, u = make_problem(args.level)
+    ne, nv = elems.shape[0], nodes.shape[0]
+    mesh = eb.Mesh(nodes, elems, ORDER)
+    pairs = mesh.far_quad_pairs
+    dev = torch.device("cuda", local)
+    st = torch.cuda.current_stream()
+    d_t = torch.from_numpy(t).to(dev)
+    d_u = torch.from_numpy(u).to(dev)
+    d_v = torch.empty(ne, dtype=torch.float64, device=dev)
+    d_q = torch.empty(ne, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def apply(prec):
+        mesh.apply_device(d_t.data_ptr(), d_u.data_ptr(), d_v.data_ptr(), d_q.data_ptr(), precision=prec,
+                          stream=st.cuda_stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def timed(prec, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            apply(prec)
+        mesh.set_profiling(True)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        far_ms = []
+        barrier()
+        ctx = sampler if sampler is not None else _Null()
+        with ctx:
+            for k in range(steps):
+                flush.zero_()  # L2 flush between timed steps (outside the events)
+                starts[k].record(st)
+                apply(prec)
+                ends[k].record(st)
+                far_ms.append(mesh.last_kernel_ms())  # syncs on this step's events
+            barrier()
+        mesh.set_profiling(False)
+        ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+        return ms, far_ms
+
+    # headline: mixed precision, device-resident inputs
+    sampler = ClockSampler(local)
+    ms_mixed, far_mixed = timed("mixed", args.steps, args.warmup, sampler)
+    v_mixed = d_v.cpu().numpy()
+    q_mixed = d_q.cpu().numpy()
+    # plain FP64 beside it (fewer steps: it is ~3x slower)
+    k64 = max(2, args.steps // 3)
+    ms_fp64, far_fp64 = timed("fp64", k64, 1)
+    v_64 = d_v.cpu().numpy()
+    q_64 = d_q.cpu().numpy()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    step_ms = max_over_ranks(sum(ms_mixed) / len(ms_mixed))
+    step_ms64 = max_over_ranks(sum(ms_fp64) / len(ms_fp64))
+    value = world * pairs / (step_ms * 1e-3) / 1e9
+    value64 = world * pairs / (step_ms64 * 1e-3) / 1e9
+
+    # e2e through the host-buffer C ABI with pinned host memory
+    h_t = torch.from_numpy(t).pin_memory()
+    h_u = torch.from_numpy(u).pin_memory()
+    h_v = torch.empty(ne, dtype=torch.float64).pin_memory()
+    h_q = torch.empty(ne, dtype=torch.float64).pin_memory()
+    import ctypes
+    L = _lib.lib()
+    P = lambda x: ctypes.c_void_p(x.data_ptr())
+    for _ in range(max(1, args.warmup)):
+        _lib.check(L.eb_apply_sl_dl(mesh.handle, 1, P(h_t), P(h_u), P(h_v), P(h_q)))
+    barrier()
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        _lib.check(L.eb_apply_sl_dl(mesh.handle, 1, P(h_t), P(h_u), P(h_v), P(h_q)))
+        e2e_times.append(time.perf_counter() - a)
+    barrier()
+    e2e_s = max_over_ranks(sum(e2e_times) / len(e2e_times))
+    e2e_value = world * pairs / e2e_s / 1e9
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # accuracy against the CPU oracle on sampled rows (same inputs)
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(5)
+    rows = np.sort(rng.choice(ne, 24, replace=False)).astype(np.int32)
+    vo, qo = Oracle(ORDER).apply_rows(nodes, elems, t, u, rows)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    err = {"mixed_sl": rel(v_mixed[rows], vo), "mixed_dl": rel(q_mixed[rows], qo),
+           "fp64_sl": rel(v_64[rows], vo), "fp64_dl": rel(q_64[rows], qo),
+           "mixed_vs_fp64_full_sl": rel(v_mixed, v_64), "mixed_vs_fp64_full_dl": rel(q_mixed, q_64),
+           "oracle_rows": len(rows)}
+
+    # roofline of the dominant kernel (far field), event-timed on its stream
+    far_avg = sum(f for f, _ in far_mixed) / len(far_mixed)
+    fin_avg = sum(g for _, g in far_mixed) / len(far_mixed)
+    peak_tflops, _ = _measure_peak()
+    achieved = pairs * FLOPS_PER_PAIR / (far_avg * 1e-3) / 1e12
+    near_bytes = 12 * mesh.near_pairs + 8 * ne * 13 * 3  # SL CSR + DL CSR values/cols (approx.)
+    cpu = None if args.no_cpu_baseline else cpu_reference_sample(nodes, elems, t, u)
+    clocks = sampler.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gpairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 far field / f64 near field", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "triangles": ne, "vertices": nv, "quad_pairs_per_step": pairs,
+                   "near_pairs": mesh.near_pairs, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "fp64": {"value": value64, "unit": "Gpairs/s", "ms_per_step": step_ms64, "steps": len(ms_fp64),
+                 "far_ms": sum(f for f, _ in far_fp64) / len(far_fp64)},
+        "mixed_over_fp64": value / value64,
+        "rel_err_vs_oracle": err,
+        "e2e": {"value": e2e_value, "unit": "Gpairs/s", "h2d_bytes_per_step": 8 * (ne + nv),
+                "d2h_bytes_per_step": 16 * ne, "ms_per_step": 1e3 * e2e_s},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                     "frac": achieved / peak_tflops if peak_tflops else None, "traffic": None,
+                     "kernel": "far_kernel<float,7,7,1,true>", "far_ms": far_avg,
+                     "flops_per_pair": FLOPS_PER_PAIR,
+                     "peak_source": "FP32 FFMA-chain calibration kernel measured in this run"},
+        "near_field": {"finalize_ms": fin_avg, "approx_bytes": near_bytes,
+                       "GB/s": near_bytes / (fin_avg * 1e-3) / 1e9 if fin_avg > 0 else None},
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def _measure_peak():
+    import ctypes
+    from easybem_b200 import _lib
+    tf, s = ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.lib().eb_measure_fp32_peak(ctypes.byref(tf), ctypes.byref(s)))
+    return tf.value, s.value
+
+
+if __name__ == "__main__":
+    main()

@@ -44,6 +44,7 @@ _SIGNATURES = {
     "eb_apply_hypersingular": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_quadrature": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp,
                                      ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]),
+    "eb_measure_fp32_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "eb_set_profiling": (ctypes.c_int, [_dp, ctypes.c_int]),
     "eb_last_kernel_ms": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
 }

@@ -98,53 +98,89 @@ static int build_static(Mesh* m)
 {
   HostMesh& h = m->h;
   const int ne = h.ne, Q = h.Q, K = h.K;
+  const int ntt = (h.nitems + kTT - 1) / kTT;
   std::vector<float4> pos32((size_t)ne * Q), tgt32((size_t)h.nitems * K);
-  std::vector<dq> pos64((size_t)ne * Q), trin(ne), tgt64((size_t)h.nitems * K), tcent(h.nitems), ccent(h.ncells);
+  std::vector<dq> pos64((size_t)ne * Q), trin(ne), tgt64((size_t)h.nitems * K), tcent(h.nitems), tnrm(h.nitems),
+      ccent(h.ncells), snrm(ne), ttile(ntt), splane64(ne);
+  std::vector<float4> splane32(ne);
+  std::vector<double> wjtab((size_t)ne * Q);
   std::vector<int4> svid(ne), tvid(h.nitems);
   std::vector<double> bary(2 * (size_t)Q);
   for (int b = 0; b < Q; b++) {
     bary[2 * b] = h.quad.tx[b];
     bary[2 * b + 1] = h.quad.ty[b];
   }
-  for (int c = 0; c < h.ncells; c++)
-    ccent[c] = dq{h.cell_center[3 * c], h.cell_center[3 * c + 1], h.cell_center[3 * c + 2], 0.0};
+  auto vertex = [&](int s, int k) {
+    const int v = h.elems[3 * h.perm[s] + k];
+    return mk3(h.nodes[3 * v], h.nodes[3 * v + 1], h.nodes[3 * v + 2]);
+  };
+  // cell bounding spheres (centre = mean centroid, radius over all vertices)
+  for (int c = 0; c < h.ncells; c++) {
+    const d3 cc = mk3(h.cell_center[3 * c], h.cell_center[3 * c + 1], h.cell_center[3 * c + 2]);
+    double r2 = 0.0;
+    for (int s = c * kCell; s < std::min(ne, (c + 1) * kCell); s++)
+      for (int k = 0; k < 3; k++) r2 = std::max(r2, dot3(vertex(s, k) - cc, vertex(s, k) - cc));
+    ccent[c] = dq{cc.x, cc.y, cc.z, std::sqrt(r2) * (1.0 + 1e-12)};
+  }
   for (int s = 0; s < ne; s++) {
-    const int i = h.perm[s];
-    const int* f = &h.elems[3 * i];
     d3 P[3];
-    for (int k = 0; k < 3; k++) P[k] = mk3(h.nodes[3 * f[k]], h.nodes[3 * f[k] + 1], h.nodes[3 * f[k] + 2]);
+    for (int k = 0; k < 3; k++) P[k] = vertex(s, k);
+    const int* f = &h.elems[3 * h.perm[s]];
     const d3 w = P[1] - P[0], z = P[2] - P[0];
     const d3 n = cross3(w, z);
     const double J = std::sqrt(dot3(n, n));
     trin[s] = dq{n.x / J, n.y / J, n.z / J, J};
+    const d3 nu = (1.0 / J) * n;
+    snrm[s] = dq{nu.x, nu.y, nu.z, dot3(P[0], nu)};
     svid[s] = make_int4(f[0], f[1], f[2], 0);
     const int cell = s / kCell;
-    const d3 cc = mk3(h.cell_center[3 * cell], h.cell_center[3 * cell + 1], h.cell_center[3 * cell + 2]);
+    const d3 cc = mk3(ccent[cell].x, ccent[cell].y, ccent[cell].z);
+    const double hp = dot3(P[0] - cc, nu);
+    splane64[s] = dq{nu.x, nu.y, nu.z, hp};
+    splane32[s] = make_float4((float)nu.x, (float)nu.y, (float)nu.z, (float)hp);
     for (int b = 0; b < Q; b++) {
       const d3 y = P[0] + h.quad.tx[b] * w + h.quad.ty[b] * z;
-      const double wj = h.quad.tw[b] * J;
-      pos64[(size_t)s * Q + b] = dq{y.x, y.y, y.z, wj};
+      wjtab[(size_t)s * Q + b] = h.quad.tw[b] * J;
       const d3 yr = y - cc;
-      pos32[(size_t)s * Q + b] = make_float4((float)yr.x, (float)yr.y, (float)yr.z, (float)wj);
+      pos64[(size_t)s * Q + b] = dq{-2.0 * yr.x, -2.0 * yr.y, -2.0 * yr.z, dot3(yr, yr)};
+      const float fx = (float)yr.x, fy = (float)yr.y, fz = (float)yr.z;
+      const double y2 = (double)fx * fx + (double)fy * fy + (double)fz * fz;
+      pos32[(size_t)s * Q + b] = make_float4(-2.0f * fx, -2.0f * fy, -2.0f * fz, (float)y2);
     }
     const d3 cen = (1.0 / 3.0) * (P[0] + P[1] + P[2]);
     for (int ch = 0; ch < h.nchunk; ch++) {
       const int item = s * h.nchunk + ch;
       tcent[item] = dq{cen.x, cen.y, cen.z, 0.0};
+      tnrm[item] = dq{nu.x, nu.y, nu.z, 0.0};
       tvid[item] = svid[s];
       for (int a = 0; a < K; a++) {
         const int pa = ch * K + a;
         const int pp = std::min(pa, Q - 1);
         const double wa = pa < Q ? h.quad.tw[pp] : 0.0;
         const d3 x = P[0] + h.quad.tx[pp] * w + h.quad.ty[pp] * z;
-        tgt64[(size_t)item * K + a] = dq{x.x, x.y, x.z, wa};
         const d3 xr = x - cen;
+        tgt64[(size_t)item * K + a] = dq{xr.x, xr.y, xr.z, wa};
         tgt32[(size_t)item * K + a] = make_float4((float)xr.x, (float)xr.y, (float)xr.z, (float)wa);
       }
     }
   }
+  // target-tile bounding spheres over the triangles of kTT consecutive items
+  for (int t = 0; t < ntt; t++) {
+    const int i0 = t * kTT, i1 = std::min(h.nitems, i0 + kTT);
+    d3 c = mk3(0, 0, 0);
+    for (int it = i0; it < i1; it++) c = c + mk3(tcent[it].x, tcent[it].y, tcent[it].z);
+    c = (1.0 / (i1 - i0)) * c;
+    double r2 = 0.0;
+    for (int it = i0; it < i1; it++)
+      for (int k = 0; k < 3; k++) {
+        const d3 v = vertex(it / h.nchunk, k);
+        r2 = std::max(r2, dot3(v - c, v - c));
+      }
+    ttile[t] = dq{c.x, c.y, c.z, std::sqrt(r2) * (1.0 + 1e-12)};
+  }
   EB_CHECK(upload(m->pos32, pos32));
   EB_CHECK(upload(m->pos64, pos64));
+  EB_CHECK(upload(m->wj, wjtab));
   EB_CHECK(upload(m->trin, trin));
   EB_CHECK(upload(m->svid, svid));
   EB_CHECK(upload(m->perm, h.perm));
@@ -153,8 +189,13 @@ static int build_static(Mesh* m)
   EB_CHECK(upload(m->tgt32, tgt32));
   EB_CHECK(upload(m->tgt64, tgt64));
   EB_CHECK(upload(m->tcent, tcent));
+  EB_CHECK(upload(m->tnrm, tnrm));
+  EB_CHECK(upload(m->snrm, snrm));
   EB_CHECK(upload(m->tvid, tvid));
   EB_CHECK(upload(m->ccent, ccent));
+  EB_CHECK(upload(m->ttile, ttile));
+  EB_CHECK(upload(m->splane32, splane32));
+  EB_CHECK(upload(m->splane64, splane64));
   return EB_OK;
 }
 
@@ -270,10 +311,15 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
     desc.tgt32 = m->tgt32.as<float4>();
     desc.tgt64 = m->tgt64.as<dq>();
     desc.tcent = m->tcent.as<dq>();
+    desc.tnrm = m->tnrm.as<dq>();
+    desc.snrm = m->snrm.as<dq>();
     desc.tvid = m->tvid.as<int4>();
     desc.rec = m->rec.p;
     desc.svid = m->svid.as<int4>();
     desc.ccent = m->ccent.as<dq>();
+    desc.ttile = m->ttile.as<dq>();
+    desc.splane32 = m->splane32.as<float4>();
+    desc.splane64 = m->splane64.as<dq>();
     desc.partial = m->partial.as<double>();
     desc.nitems = h.nitems;
     desc.ne = h.ne;
@@ -292,7 +338,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
     var.src_tile = desc.src_tile;
   }
   const void* pos = fp32 ? m->pos32.p : m->pos64.p;
-  EB_CUDA(prep_launch(fp32, nsl, dl, h.ne, h.Q, pos, m->trin.as<dq>(), m->svid.as<int4>(), m->perm.as<int>(),
+  EB_CUDA(prep_launch(fp32, nsl, dl, h.ne, h.Q, pos, m->wj.as<double>(), m->svid.as<int4>(), m->perm.as<int>(),
                       m->bary.as<double>(), d_t, h.ne, d_u, m->rec.p, st));
   EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
   if (m->profile) {

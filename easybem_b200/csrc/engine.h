@@ -14,9 +14,9 @@ cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshD
                        int* dc, size_t smem, int grid, cudaStream_t st);
 int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem);
 bool far_variant_supported(int NSL, bool DL);
-cudaError_t prep_launch(bool fp32, int NSL, bool DL, int ne, int Q, const void* pos, const dq* trin, const int4* svid,
-                        const int* perm, const double* bary, const double* t, int tstride, const double* u, void* rec,
-                        cudaStream_t st);
+cudaError_t prep_launch(bool fp32, int NSL, bool DL, int ne, int Q, const void* pos, const double* wj,
+                        const int4* svid, const int* perm, const double* bary, const double* t, int tstride,
+                        const double* u, void* rec, cudaStream_t st);
 cudaError_t finalize_launch(int NSL, bool DL, int ne, int nchunk, int nsplit, int nitems, const int* iperm,
                             const dq* trin, const double* partial, const int* sl_rowptr, const int* sl_col,
                             const double* sl_val, const int* dl_rowptr, const int* dl_col, const double* dl_val,
@@ -52,8 +52,8 @@ struct Mesh {
   int device = 0;
 
   // static geometry (sorted order)
-  DevBuf pos32, pos64, trin, svid, perm, iperm, bary;
-  DevBuf tgt32, tgt64, tcent, tvid, ccent;
+  DevBuf pos32, pos64, wj, trin, svid, perm, iperm, bary;
+  DevBuf tgt32, tgt64, tcent, tnrm, tvid, ccent, snrm, ttile, splane32, splane64;
   // near field
   DevBuf sl_rowptr, sl_col, sl_val, dl_rowptr, dl_col, dl_val;
   long long npairs = 0;

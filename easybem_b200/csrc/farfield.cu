@@ -6,7 +6,25 @@
 #include "farfield.cuh"
 #include "mesh_host.h"
 
+// Launch shape of the far-field kernel: minimum resident CTAs per SM (which
+// caps registers per thread) and the unroll depth of the source-point loop.
+#ifndef EB_F32_MINB
+#define EB_F32_MINB 3
+#endif
+#ifndef EB_F64_MINB
+#define EB_F64_MINB 2
+#endif
+#ifndef EB_UNROLL_B_F32
+#define EB_UNROLL_B_F32 0  // 0: unroll fully when the rule size is a compile-time constant
+#endif
+#ifndef EB_UNROLL_B_F64
+#define EB_UNROLL_B_F64 1
+#endif
+
 namespace eb {
+
+constexpr int kUnrollF32 = EB_UNROLL_B_F32;
+constexpr int kUnrollF64 = EB_UNROLL_B_F64;
 
 // Neumann/Knuth two-sum accumulation: (s, e) holds s + e exactly up to the
 // rounding of e.
@@ -38,68 +56,112 @@ struct Slot<double> {
 
 __device__ __forceinline__ float comp(const float4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
 __device__ __forceinline__ double comp(const dq& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
-__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+// One MUFU.RSQ (the argument is a squared distance, never denormal).
+__device__ __forceinline__ float rsq(float x)
+{
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
 
-// One source point against the K target points of an item.
-template <typename T, int K, int NSL, bool DL, typename S>
-__device__ __forceinline__ void eval_point(const S* __restrict__ r, const T (&x)[K], const T (&y)[K],
-                                           const T (&z)[K], T (&sl)[NSL > 0 ? NSL : 1][K], T (&dl)[K])
+// FP64 1/sqrt: the PTX approximation refined by one Halley step
+// (y' = y (1 + e/2 + 3e^2/8), e = 1 - x y^2), cubic convergence.
+__device__ __forceinline__ double rsq_f64(double x)
 {
-  constexpr int NREC = rec_slots(NSL, DL);
-  const S p0 = r[0];
-  S p1;
-  if constexpr (DL || NSL > 1) p1 = r[1];
-#pragma unroll
-  for (int a = 0; a < K; ++a) {
-    const T dx = x[a] - p0.x, dy = y[a] - p0.y, dz = z[a] - p0.z;
-    const T r2 = dx * dx + dy * dy + dz * dz;
-    const T inv = rsq(r2);
-    if constexpr (NSL >= 1) sl[0][a] += p0.w * inv;
-#pragma unroll
-    for (int c = 1; c < NSL; ++c) {
-      int slot, cc;
-      charge_slot(c, DL, &slot, &cc);
-      sl[c][a] += comp(slot == 1 ? p1 : r[slot], cc) * inv;
-    }
-    if constexpr (DL) {
-      const T rp = dx * p1.x + dy * p1.y + dz * p1.z;
-      const T inv2 = inv * inv;
-      dl[a] += (rp * inv2) * inv;
-    }
-  }
-  (void)NREC;
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x * y, y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
 }
 
-// One target item against the source points of triangles [s0, s1) of the
-// staged tile: accumulates SL charges (NSL of them) and the DL dipole term.
-// Source triangles sharing a vertex with the target triangle are skipped.
-template <typename T, int K, int NQ, int NSL, bool DL>
-__device__ __forceinline__ void eval_segment(const typename Slot<T>::type* __restrict__ srec,
-                                             const int4* __restrict__ svid, int s0, int s1, int nq,
-                                             int4 tv, const T (&x)[K], const T (&y)[K], const T (&z)[K],
-                                             T (&sl)[NSL > 0 ? NSL : 1][K], T (&dl)[K])
+// One target item (K points) against the source triangles [s0, s1) of one
+// cell of the staged tile. Per quadrature-point pair:
+//   SL:  sl[c][a] += c_c(b) / r
+//   DL:  acc[a]   += s(b) / r^3          (per source triangle)
+// and per source triangle dl[a] += d(a, j) * acc[a], where d(a, j) =
+// (x_a - y).n_j is the signed distance of x_a from the plane of triangle j
+// (the same for every y in it), evaluated as d = (x_a - c_i).(n_j - n_i) +
+// (c_i.n_j - P0_j.n_j) with the normal difference and the centroid term formed
+// in FP64, so the small normal component is not lost to cancellation
+// ((x_a - c_i) enters as the cell-relative point plus the cell offset o).
+// FAR: cell well separated from the whole target tile (no vertex mask,
+// expanded |x - y|^2, d from the cell-relative plane offset (P0_j - c_cell).n_j
+// in the working precision); otherwise the shared-vertex mask and direct
+// differences.
+template <typename T, int K, int NQ, int NSL, bool DL, bool FAR>
+__device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restrict__ srec,
+                                          const int4* __restrict__ svid, const dq* __restrict__ snrm,
+                                          const typename Slot<T>::type* __restrict__ splane, int s0,
+                                          int s1, int nq, int4 tv, const T (&x)[K], const T (&y)[K],
+                                          const T (&z)[K], const T (&q2)[K], const T (&o)[3],
+                                          const double (&cen)[3], const double (&nrm)[3],
+                                          T (&sl)[NSL > 0 ? NSL : 1][K], T (&dl)[K])
 {
+  using S = typename Slot<T>::type;
   constexpr int NREC = rec_slots(NSL, DL);
+  constexpr int kUnroll = std::is_same<T, float>::value ? kUnrollF32 : kUnrollF64;
+  const int nqr = NQ > 0 ? NQ : nq;
 #pragma unroll 1
   for (int s = s0; s < s1; ++s) {
-    if (shares_vertex(tv, svid[s])) continue;
-    if constexpr (NQ > 0) {
-      const typename Slot<T>::type* r = srec + (size_t)s * NQ * NREC;
+    if constexpr (!FAR) {
+      if (shares_vertex(tv, svid[s])) continue;
+    }
+    const S* r = srec + (size_t)s * nqr * NREC;
+    T acc[K];
 #pragma unroll
-      for (int b = 0; b < NQ; ++b) eval_point<T, K, NSL, DL>(r + b * NREC, x, y, z, sl, dl);
-    } else {
-      const typename Slot<T>::type* r = srec + (size_t)s * nq * NREC;
-#pragma unroll 1
-      for (int b = 0; b < nq; ++b) eval_point<T, K, NSL, DL>(r + b * NREC, x, y, z, sl, dl);
+    for (int a = 0; a < K; ++a) acc[a] = 0;
+#pragma unroll(NQ > 0 ? (kUnroll > 0 ? kUnroll : NQ) : 1)
+    for (int b = 0; b < nqr; ++b) {
+      const S p0 = r[b * NREC];
+      const S p1 = r[b * NREC + 1];
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        T r2;
+        if constexpr (FAR) {
+          r2 = x[a] * p0.x + (y[a] * p0.y + (z[a] * p0.z + (q2[a] + p0.w)));
+        } else {
+          const T dx = x[a] + T(0.5) * p0.x, dy = y[a] + T(0.5) * p0.y, dz = z[a] + T(0.5) * p0.z;
+          r2 = dx * dx + dy * dy + dz * dz;
+        }
+        T inv;
+        if constexpr (std::is_same<T, float>::value) inv = rsq(r2);
+        else inv = rsq_f64(r2);
+#pragma unroll
+        for (int c = 0; c < NSL; ++c) {
+          constexpr bool dlc = DL;
+          const int slot = charge_slot(c, dlc);
+          sl[c][a] += comp(slot == 1 ? p1 : r[b * NREC + slot], charge_comp(c, dlc)) * inv;
+        }
+        if constexpr (DL) acc[a] += (inv * inv) * (p1.x * inv);
+      }
+    }
+    if constexpr (DL && FAR) {
+      // well-separated pair: d = (x_a - c_cell).n_j - (P0_j - c_cell).n_j
+      const typename Slot<T>::type pn = splane[s];
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        const T d = x[a] * pn.x + (y[a] * pn.y + (z[a] * pn.z - pn.w));
+        dl[a] += d * acc[a];
+      }
+    } else if constexpr (DL) {
+      // x_a - c_i = (x_a - c_cell) + o with o = c_cell - c_i
+      const dq nj = snrm[s];
+      const T dnx = (T)(nj.x - nrm[0]), dny = (T)(nj.y - nrm[1]), dnz = (T)(nj.z - nrm[2]);
+      const T e = (T)(cen[0] * nj.x + cen[1] * nj.y + cen[2] * nj.z - nj.w) + (o[0] * dnx + (o[1] * dny + o[2] * dnz));
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        const T d = x[a] * dnx + (y[a] * dny + (z[a] * dnz + e));
+        dl[a] += d * acc[a];
+      }
     }
   }
 }
 
 template <typename T, int K, int NQ, int NSL, bool DL>
-__global__ void __launch_bounds__(kTT) far_kernel(const FarMeshDesc* __restrict__ meshes,
-                                                  const WorkItem* __restrict__ items, int nitems,
-                                                  int* __restrict__ counter)
+__global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MINB : EB_F64_MINB)
+    far_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
+               int* __restrict__ counter)
 {
   using S = typename Slot<T>::type;
   constexpr bool F32 = std::is_same<T, float>::value;
@@ -108,6 +170,8 @@ __global__ void __launch_bounds__(kTT) far_kernel(const FarMeshDesc* __restrict_
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ int4 s_vid[kTS];
+  __shared__ dq s_nrm[DL ? kTS : 1];
+  __shared__ S s_plane[DL ? kTS : 1];
 
   S* s_rec = reinterpret_cast<S*>(smem_raw);
 
@@ -123,24 +187,28 @@ __global__ void __launch_bounds__(kTT) far_kernel(const FarMeshDesc* __restrict_
     const int ti = w.tgt0 + threadIdx.x;
     const bool active = ti < md.nitems;
     const int tsel = active ? ti : w.tgt0;
+    const dq tile = md.ttile[w.tgt0 / kTT];
 
-    T xt[K], yt[K], zt[K], wt[K];
-    double cx = 0.0, cy = 0.0, cz = 0.0;
-    if constexpr (F32) {
+    // target points relative to the triangle centroid are re-read per cell
+    // (L1-resident) rather than held in registers
+    double cen[3], nrm[3] = {0.0, 0.0, 0.0};
+    {
       const dq c = md.tcent[tsel];
-      cx = c.x; cy = c.y; cz = c.z;
-#pragma unroll
-      for (int a = 0; a < K; ++a) {
-        const float4 p = md.tgt32[(size_t)tsel * K + a];
-        xt[a] = p.x; yt[a] = p.y; zt[a] = p.z; wt[a] = p.w;
-      }
-    } else {
-#pragma unroll
-      for (int a = 0; a < K; ++a) {
-        const dq p = md.tgt64[(size_t)tsel * K + a];
-        xt[a] = (T)p.x; yt[a] = (T)p.y; zt[a] = (T)p.z; wt[a] = (T)p.w;
+      cen[0] = c.x; cen[1] = c.y; cen[2] = c.z;
+      if constexpr (DL) {
+        const dq n = md.tnrm[tsel];
+        nrm[0] = n.x; nrm[1] = n.y; nrm[2] = n.z;
       }
     }
+    auto target = [&](int a, T& px, T& py, T& pz, T& pw) {
+      if constexpr (F32) {
+        const float4 p = md.tgt32[(size_t)tsel * K + a];
+        px = p.x; py = p.y; pz = p.z; pw = p.w;
+      } else {
+        const dq p = md.tgt64[(size_t)tsel * K + a];
+        px = p.x; py = p.y; pz = p.z; pw = p.w;
+      }
+    };
     const int4 tv = active ? md.tvid[tsel] : make_int4(-1, -1, -1, 0);
 
     // float-float accumulators (FP32) or plain doubles (FP64) per output
@@ -157,21 +225,33 @@ __global__ void __launch_bounds__(kTT) far_kernel(const FarMeshDesc* __restrict_
       const S* g = grec + (size_t)t0 * nq * NREC;
       const int nslot = ns * nq * NREC;
       for (int k = threadIdx.x; k < nslot; k += kTT) s_rec[k] = g[k];
-      for (int k = threadIdx.x; k < ns; k += kTT) s_vid[k] = md.svid[t0 + k];
+      for (int k = threadIdx.x; k < ns; k += kTT) {
+        s_vid[k] = md.svid[t0 + k];
+        if constexpr (DL) {
+          s_nrm[k] = md.snrm[t0 + k];
+          if constexpr (F32) s_plane[k] = md.splane32[t0 + k];
+          else s_plane[k] = md.splane64[t0 + k];
+        }
+      }
       __syncthreads();
       if (active) {
         for (int g0 = 0; g0 < ns;) {
           const int cell = (t0 + g0) / kCell;
           const int g1 = min(ns, (cell + 1) * kCell - t0);
-          T xs[K], ys[K], zs[K];
-          if constexpr (F32) {
-            const dq cc = md.ccent[cell];
-            const float ox = (float)(cc.x - cx), oy = (float)(cc.y - cy), oz = (float)(cc.z - cz);
+          const dq cc = md.ccent[cell];
+          // warp-uniform (tile-level) separation test
+          const double ddx = cc.x - tile.x, ddy = cc.y - tile.y, ddz = cc.z - tile.z;
+          const double rr = kFarRatio * (cc.w + tile.w);
+          const bool far = ddx * ddx + ddy * ddy + ddz * ddz > rr * rr;
+          // targets relative to the cell centre
+          const T o[3] = {(T)(cc.x - cen[0]), (T)(cc.y - cen[1]), (T)(cc.z - cen[2])};
+          T xs[K], ys[K], zs[K], q2[K];
 #pragma unroll
-            for (int a = 0; a < K; ++a) { xs[a] = xt[a] - ox; ys[a] = yt[a] - oy; zs[a] = zt[a] - oz; }
-          } else {
-#pragma unroll
-            for (int a = 0; a < K; ++a) { xs[a] = xt[a]; ys[a] = yt[a]; zs[a] = zt[a]; }
+          for (int a = 0; a < K; ++a) {
+            T px, py, pz, pw;
+            target(a, px, py, pz, pw);
+            xs[a] = px - o[0]; ys[a] = py - o[1]; zs[a] = pz - o[2];
+            q2[a] = xs[a] * xs[a] + ys[a] * ys[a] + zs[a] * zs[a];
           }
           T sl[NS][K], dl[K];
 #pragma unroll
@@ -180,14 +260,23 @@ __global__ void __launch_bounds__(kTT) far_kernel(const FarMeshDesc* __restrict_
 #pragma unroll
             for (int c = 0; c < NS; ++c) sl[c][a] = 0;
           }
-          eval_segment<T, K, NQ, NSL, DL>(s_rec, s_vid, g0, g1, nq, tv, xs, ys, zs, sl, dl);
+          if (far)
+            eval_cell<T, K, NQ, NSL, DL, true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+                                               nrm, sl, dl);
+          else
+            eval_cell<T, K, NQ, NSL, DL, false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
+                                                cen, nrm, sl, dl);
 #pragma unroll
           for (int c = 0; c <= NS; ++c) {
             if (c == NS && !DL) break;
             if (c < NS && NSL == 0) continue;
             T part = 0;
 #pragma unroll
-            for (int a = 0; a < K; ++a) part += wt[a] * (c < NS ? sl[c][a] : dl[a]);
+            for (int a = 0; a < K; ++a) {
+              T px, py, pz, pw;
+              target(a, px, py, pz, pw);
+              part += pw * (c < NS ? sl[c][a] : dl[a]);
+            }
             if constexpr (F32) two_sum_add(acc_hi[c], acc_lo[c], part);
             else acc_hi[c] += part;
           }
@@ -207,10 +296,10 @@ __global__ void __launch_bounds__(kTT) far_kernel(const FarMeshDesc* __restrict_
 }
 
 // Source records for one apply: positions (static) with the per-apply
-// charges w_b J_j t_j and dipoles w_b J_j u_h(y_b) n_j.
+// strengths s = w_b J_j u_h(y_b) (DL) and charges c_r = w_b J_j t_r[j] (SL).
 template <typename T, int NSL, bool DL>
 __global__ void prep_kernel(int ne, int Q, const typename Slot<T>::type* __restrict__ pos,
-                            const dq* __restrict__ trin, const int4* __restrict__ svid,
+                            const double* __restrict__ wj_tab, const int4* __restrict__ svid,
                             const int* __restrict__ perm, const double* __restrict__ bary,
                             const double* __restrict__ t, int tstride, const double* __restrict__ u,
                             typename Slot<T>::type* __restrict__ rec)
@@ -220,31 +309,26 @@ __global__ void prep_kernel(int ne, int Q, const typename Slot<T>::type* __restr
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)ne * Q) return;
   const int j = (int)(idx / Q), b = (int)(idx % Q);
-  const S p = pos[idx];
-  const double wj = (double)p.w;  // w_b * J_j (rounded to T in the FP32 table)
-  S* r = rec + idx * NREC;
-  S s0;
-  s0.x = p.x; s0.y = p.y; s0.z = p.z; s0.w = 0;
+  const double wj = wj_tab[idx];  // w_b * J_j
   const int orig = perm[j];
-  if (NSL >= 1) s0.w = (T)(wj * t[orig]);
-  r[0] = s0;
-  if (DL) {
-    const dq n = trin[j];
+  T vals[4 * NREC];
+#pragma unroll
+  for (int k = 0; k < 4 * NREC; ++k) vals[k] = 0;
+#pragma unroll
+  for (int c = 0; c < NSL; ++c) vals[4 * charge_slot(c, DL) + charge_comp(c, DL)] = (T)(wj * t[(size_t)c * tstride + orig]);
+  if constexpr (DL) {
     const int4 v = svid[j];
     const double e1 = bary[2 * b], e2 = bary[2 * b + 1];
     const double uh = (1.0 - e1 - e2) * u[v.x] + e1 * u[v.y] + e2 * u[v.z];
-    const double s = wj * uh;
-    S s1;
-    s1.x = (T)(s * n.x); s1.y = (T)(s * n.y); s1.z = (T)(s * n.z); s1.w = 0;
-    if (NSL >= 2) s1.w = (T)(wj * t[(size_t)tstride + orig]);
-    r[1] = s1;
+    vals[4] = (T)(wj * uh);
   }
-  for (int c = DL ? 2 : 1; c < NSL; ++c) {
-    int slot, cc;
-    charge_slot(c, DL, &slot, &cc);
-    T* rr = reinterpret_cast<T*>(&r[slot]);
-    if (cc == 0) { r[slot].x = 0; r[slot].y = 0; r[slot].z = 0; r[slot].w = 0; }
-    rr[cc] = (T)(wj * t[(size_t)c * tstride + orig]);
+  S* r = rec + idx * NREC;
+  r[0] = pos[idx];
+#pragma unroll
+  for (int k = 1; k < NREC; ++k) {
+    S o;
+    o.x = vals[4 * k]; o.y = vals[4 * k + 1]; o.z = vals[4 * k + 2]; o.w = vals[4 * k + 3];
+    r[k] = o;
   }
 }
 
@@ -391,7 +475,7 @@ int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem)
 }
 
 template <typename T>
-static cudaError_t prep_launch_t(int NSL, bool DL, int ne, int Q, const void* pos, const dq* trin, const int4* svid,
+static cudaError_t prep_launch_t(int NSL, bool DL, int ne, int Q, const void* pos, const double* wj, const int4* svid,
                                  const int* perm, const double* bary, const double* t, int tstride, const double* u,
                                  void* rec, cudaStream_t st)
 {
@@ -402,21 +486,21 @@ static cudaError_t prep_launch_t(int NSL, bool DL, int ne, int Q, const void* po
   const S* p = reinterpret_cast<const S*>(pos);
   S* r = reinterpret_cast<S*>(rec);
   switch (NSL * 2 + (DL ? 1 : 0)) {
-    case 1: prep_kernel<T, 0, true><<<grid, blk, 0, st>>>(ne, Q, p, trin, svid, perm, bary, t, tstride, u, r); break;
-    case 2: prep_kernel<T, 1, false><<<grid, blk, 0, st>>>(ne, Q, p, trin, svid, perm, bary, t, tstride, u, r); break;
-    case 3: prep_kernel<T, 1, true><<<grid, blk, 0, st>>>(ne, Q, p, trin, svid, perm, bary, t, tstride, u, r); break;
-    case 8: prep_kernel<T, 4, false><<<grid, blk, 0, st>>>(ne, Q, p, trin, svid, perm, bary, t, tstride, u, r); break;
+    case 1: prep_kernel<T, 0, true><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
+    case 2: prep_kernel<T, 1, false><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
+    case 3: prep_kernel<T, 1, true><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
+    case 8: prep_kernel<T, 4, false><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
-cudaError_t prep_launch(bool fp32, int NSL, bool DL, int ne, int Q, const void* pos, const dq* trin, const int4* svid,
-                        const int* perm, const double* bary, const double* t, int tstride, const double* u, void* rec,
-                        cudaStream_t st)
+cudaError_t prep_launch(bool fp32, int NSL, bool DL, int ne, int Q, const void* pos, const double* wj,
+                        const int4* svid, const int* perm, const double* bary, const double* t, int tstride,
+                        const double* u, void* rec, cudaStream_t st)
 {
-  return fp32 ? prep_launch_t<float>(NSL, DL, ne, Q, pos, trin, svid, perm, bary, t, tstride, u, rec, st)
-              : prep_launch_t<double>(NSL, DL, ne, Q, pos, trin, svid, perm, bary, t, tstride, u, rec, st);
+  return fp32 ? prep_launch_t<float>(NSL, DL, ne, Q, pos, wj, svid, perm, bary, t, tstride, u, rec, st)
+              : prep_launch_t<double>(NSL, DL, ne, Q, pos, wj, svid, perm, bary, t, tstride, u, rec, st);
 }
 
 cudaError_t finalize_launch(int NSL, bool DL, int ne, int nchunk, int nsplit, int nitems, const int* iperm,

@@ -40,31 +40,38 @@ struct __align__(16) dq {
   double x, y, z, w;
 };
 
-// Number of 16/32-byte record slots per source point.
-__host__ __device__ constexpr int rec_slots(int nsl, bool dl)
-{
-  return 1 + (dl ? 1 : 0) + ((nsl - (dl ? 2 : 1)) > 0 ? ((nsl - (dl ? 2 : 1)) + 3) / 4 : 0);
-}
+// Source-point record layout (FP32: float4 slots, FP64: dq slots):
+//   slot0 = (-2 y, |y|^2), y the quadrature point relative to its cell centre;
+//   slot1.. = the strengths [s (with DL), c_0, c_1, ...], four per slot, where
+//   c_r = w_b J_j t_r[j] are the SL charges and s = w_b J_j u_h(y_b) the DL
+//   strength. Far cells use |x - y|^2 = |x|^2 + |y|^2 - 2 x.y directly from
+//   slot0; near cells recover y = -(1/2)(-2y) exactly.
+__host__ __device__ constexpr int rec_slots(int nsl, bool dl) { return 1 + (nsl + (dl ? 1 : 0) + 3) / 4; }
 
-// Slot and component of charge r in a record.
-__host__ __device__ inline void charge_slot(int r, bool dl, int* slot, int* comp)
-{
-  if (r == 0) { *slot = 0; *comp = 3; return; }
-  if (r == 1 && dl) { *slot = 1; *comp = 3; return; }
-  const int k = r - (dl ? 2 : 1);
-  *slot = (dl ? 2 : 1) + k / 4;
-  *comp = k % 4;
-}
+// Slot and component of SL charge r (the DL strength is slot 1, component 0).
+__host__ __device__ constexpr int charge_slot(int r, bool dl) { return 1 + (r + (dl ? 1 : 0)) / 4; }
+__host__ __device__ constexpr int charge_comp(int r, bool dl) { return (r + (dl ? 1 : 0)) % 4; }
+
+// A source cell is "far" from a target tile when the distance of their
+// bounding-sphere centres exceeds kFarRatio times the sum of the radii (which
+// bound every vertex): no shared vertex is possible and |x|^2 + |y|^2 - 2 x.y
+// loses at most a few ulps to cancellation there.
+constexpr double kFarRatio = 2.5;
 
 // Per-mesh view used by the far-field kernels (device pointers).
 struct FarMeshDesc {
   const float4* tgt32;  // [nitems*K]: (x_a - centroid) in FP32, weight w_a
-  const dq* tgt64;      // [nitems*K]: x_a in FP64, weight w_a
+  const dq* tgt64;      // [nitems*K]: (x_a - centroid) in FP64, weight w_a
   const dq* tcent;      // [nitems]: centroid of the item's triangle (FP64)
+  const dq* tnrm;       // [nitems]: unit normal of the item's triangle (FP64)
+  const dq* snrm;       // [ne]: unit normal n_j and plane offset P0_j . n_j of sorted sources
+  const float4* splane32;  // [ne]: n_j and (P0_j - c_cell) . n_j in FP32 (far cells)
+  const dq* splane64;      // [ne]: the same in FP64
   const int4* tvid;     // [nitems]: vertex ids of the item's triangle (-1 if padding)
   const void* rec;      // [ne*Q*nrec] source records (float4 or dq), sorted order
   const int4* svid;     // [ne]: vertex ids of sorted source triangles
-  const dq* ccent;      // [ncells]: cell centres (FP64)
+  const dq* ccent;      // [ncells]: cell centre and bounding radius (FP64)
+  const dq* ttile;      // [ntiles]: target-tile centre and bounding radius (FP64)
   double* partial;      // [nout][nsplit][nitems]
   int nitems, ne, Q, nsplit, src_tile;
 };

@@ -85,6 +85,11 @@ int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double*
 int eb_quadrature(int order, int* nline, double* lx, double* lw, int* ntri, double* tx, double* ty,
                   double* tw);
 
+/* Roofline calibration: sustained FP32 FFMA throughput of the current GPU in
+ * TFLOP/s (FMA = 2 flops), from a register-only FMA-chain kernel. No
+ * counterpart in the reference. */
+int eb_measure_fp32_peak(double* tflops, double* seconds);
+
 /* Event timing of the far-field kernel and of the finalize kernel (which
  * includes the near-field SpMV) of the last apply on this mesh, recorded on
  * the apply's stream when profiling is on. Blocks until that apply ends.
