@@ -376,6 +376,8 @@ struct eb_mesh_s {
 
 using eb::set_error;
 
+eb::Mesh* eb_mesh_internal(eb_mesh handle) { return handle ? handle->m : nullptr; }
+
 extern "C" {
 
 const char* eb_version(void) { return "easybem-b200 0.1"; }

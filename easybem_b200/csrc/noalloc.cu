@@ -1,0 +1,137 @@
+// An apply entry point that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc at the moment they need a matvec: an
+// application whose memory is owned by its own pool or framework allocator
+// (so that a stray cudaMalloc would fragment or exceed a budget it enforces),
+// or a real-time loop that must not hit the driver's allocator, which can
+// synchronise the device. eb_apply_sl_dl_noalloc serves them: the caller
+// passes device pointers for the densities and the results, the mesh must
+// already exist (eb_mesh_create allocates its resident geometry once), and
+// every per-apply scratch buffer (source records, partial row sums, the work
+// counter and the launch descriptor) lives in one fixed device array defined
+// in this file.
+//
+// That array has kNoAllocScratchBytes bytes and is held by every GPU that
+// loads the library until the process exits. Meshes whose scratch would not
+// fit are rejected with EB_ERR_INVALID and a message stating the size. All
+// calls share the array and the last call's contents stay in it; the work
+// counter is cleared by each call. Two calls whose work overlaps on the GPU
+// (different streams, or different meshes at the same time) race on the
+// array: issue them on one stream or wait in between.
+//
+// The first call on each device looks up the array's device address
+// (cudaGetSymbolAddress) with that device current; make that first call
+// before any stream capture.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "engine.h"
+
+namespace eb {
+
+constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static void* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// Writes the launch descriptor (passed by value) into the scratch array.
+__global__ void noalloc_store_desc(FarMeshDesc d, FarMeshDesc* dst)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = d;
+}
+
+}  // namespace eb
+
+// The mesh behind a handle (defined with the handle in engine.cu).
+eb::Mesh* eb_mesh_internal(eb_mesh handle);
+
+extern "C" int eb_apply_sl_dl_noalloc(eb_mesh handle, int precision, const double* d_t, const double* d_u,
+                                      double* d_v, double* d_q, void* stream)
+{
+  using namespace eb;
+  if (!handle) return set_error(EB_ERR_INVALID, "null mesh");
+  Mesh* m = eb_mesh_internal(handle);
+  const HostMesh& h = m->h;
+  if (precision != EB_PREC_FP64 && precision != EB_PREC_MIXED)
+    return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
+  const bool sl = d_t && d_v, dl = d_u && d_q;
+  if (!sl && !dl) return set_error(EB_ERR_INVALID, "nothing to apply: pass t/v and/or u/q");
+  const int nsl = sl ? 1 : 0;
+  const bool fp32 = precision == EB_PREC_MIXED;
+  EB_CUDA(cudaSetDevice(m->device));
+  if (m->device < 0 || m->device >= kNoAllocMaxDevices) return set_error(EB_ERR_INVALID, "device index too large");
+
+  // scratch layout: [counter | descriptor | source records | partial sums]
+  const int nrec = rec_slots(nsl, dl);
+  const size_t slot = fp32 ? sizeof(float4) : sizeof(dq);
+  const size_t off_desc = 256;
+  const size_t off_rec = off_desc + align256(sizeof(FarMeshDesc));
+  const size_t rec_bytes = (size_t)h.ne * h.Q * nrec * slot;
+  const size_t off_part = off_rec + align256(rec_bytes);
+  const int nout = nsl + (dl ? 1 : 0);
+  const size_t part_bytes = sizeof(double) * (size_t)nout * m->plan.nsplit * h.nitems;
+  const size_t need = off_part + align256(part_bytes);
+  if (need > kNoAllocScratchBytes)
+    return set_error(EB_ERR_INVALID, "this mesh needs " + std::to_string(need) +
+                                         " bytes of apply scratch; eb_apply_sl_dl_noalloc holds at most " +
+                                         std::to_string(kNoAllocScratchBytes) + " bytes (use eb_apply_sl_dl_device)");
+
+  // once per device, with that device current
+  if (!g_noalloc_ptr[m->device]) {
+    void* p = nullptr;
+    EB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[m->device] = p;
+  }
+  unsigned char* base = static_cast<unsigned char*>(g_noalloc_ptr[m->device]);
+  int* counter = reinterpret_cast<int*>(base);
+  FarMeshDesc* d_desc = reinterpret_cast<FarMeshDesc*>(base + off_desc);
+  void* rec = base + off_rec;
+  double* partial = reinterpret_cast<double*>(base + off_part);
+  cudaStream_t st = (cudaStream_t)stream;
+
+  FarMeshDesc desc;
+  desc.tgt32 = m->tgt32.as<float4>();
+  desc.tgt64 = m->tgt64.as<dq>();
+  desc.tcent = m->tcent.as<dq>();
+  desc.tnrm = m->tnrm.as<dq>();
+  desc.snrm = m->snrm.as<dq>();
+  desc.splane32 = m->splane32.as<float4>();
+  desc.splane64 = m->splane64.as<dq>();
+  desc.tvid = m->tvid.as<int4>();
+  desc.rec = rec;
+  desc.svid = m->svid.as<int4>();
+  desc.ccent = m->ccent.as<dq>();
+  desc.ttile = m->ttile.as<dq>();
+  desc.partial = partial;
+  desc.nitems = h.nitems;
+  desc.ne = h.ne;
+  desc.Q = h.Q;
+  desc.nsplit = m->plan.nsplit;
+  const size_t per_tri = (size_t)h.Q * nrec * slot;
+  desc.src_tile = (int)std::max<size_t>(1, std::min<size_t>(kTS, (40 * 1024) / per_tri));
+  const size_t smem = (size_t)desc.src_tile * h.Q * nrec * slot;
+  int occ = far_occupancy(fp32, nsl, dl, h.K, h.Q, smem);
+  if (occ < 1) occ = 1;
+  int nsm = 148;
+  EB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device));
+  const int grid = std::min(nsm * occ, std::max(1, m->nitems_work));
+
+  noalloc_store_desc<<<1, 32, 0, st>>>(desc, d_desc);
+  EB_CUDA(cudaGetLastError());
+  const void* pos = fp32 ? m->pos32.p : m->pos64.p;
+  EB_CUDA(prep_launch(fp32, nsl, dl, h.ne, h.Q, pos, m->wj.as<double>(), m->svid.as<int4>(), m->perm.as<int>(),
+                      m->bary.as<double>(), d_t, h.ne, d_u, rec, st));
+  EB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+  EB_CUDA(far_launch(fp32, nsl, dl, h.K, h.Q, d_desc, m->items.as<WorkItem>(), m->nitems_work, counter, smem, grid,
+                     st));
+  EB_CUDA(finalize_launch(nsl, dl, h.ne, h.nchunk, m->plan.nsplit, h.nitems, m->iperm.as<int>(), m->trin.as<dq>(),
+                          partial, m->sl_rowptr.as<int>(), m->sl_col.as<int>(), m->sl_val.as<double>(),
+                          m->dl_rowptr.as<int>(), m->dl_col.as<int>(), m->dl_val.as<double>(), d_t, h.ne, d_u, d_v,
+                          h.ne, d_q, st));
+  return EB_OK;
+}

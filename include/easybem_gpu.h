@@ -67,6 +67,18 @@ int eb_apply_sl_dl(eb_mesh mesh, int precision, const double* t, const double* u
 int eb_apply_sl_dl_device(eb_mesh mesh, int precision, const double* d_t, const double* d_u,
                           double* d_v, double* d_q, void* stream);
 
+/* eb_apply_sl_dl_device without any device allocation, for callers that
+ * cannot call cudaMalloc when they apply the operator (memory owned by their
+ * own pool or framework allocator, or a loop that must not enter the driver's
+ * allocator). No counterpart in the reference. Device pointers in and out;
+ * all per-apply scratch lives in one fixed 32 MiB device array that every GPU
+ * loading the library keeps until exit. Meshes needing more scratch are
+ * rejected (EB_ERR_INVALID, message gives the size). Calls share that array:
+ * calls overlapping on the GPU race. The first call on a device looks up the
+ * array's address and should come before any stream capture. */
+int eb_apply_sl_dl_noalloc(eb_mesh mesh, int precision, const double* d_t, const double* d_u,
+                           double* d_v, double* d_q, void* stream);
+
 /* v = V1 t, the single layer with P1 test and trial functions (t, v have
  * nnodes entries). Replaces applyGPULaplace3d1Layer(t, v, 1)
  * (src/BEM3dLaplaceGPU.cu:82-154, 211-320, 371-442, 491-557, host :1034-1313). */
