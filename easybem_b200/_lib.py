@@ -43,6 +43,7 @@ _SIGNATURES = {
     "eb_apply_sl_dl_noalloc": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]),
     "eb_apply_sl_p1": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_apply_hypersingular": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_apply_hypersingular_device": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp]),
     "eb_quadrature": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp,
                                      ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]),
     "eb_measure_fp32_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),

@@ -452,7 +452,7 @@ static int host_apply(eb_mesh mesh, int precision, const double* t, const double
   }
   if (dl) {
     EB_CHECK(m->io_u.alloc(sizeof(double) * nv));
-    EB_CHECK(m->io_q.alloc(sizeof(double) * ne));
+    EB_CHECK(m->io_q.alloc(sizeof(double) * std::max(ne, nv)));
     EB_CUDA(cudaMemcpyAsync(m->io_u.p, u, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
   }
   EB_CHECK(eb::mesh_apply(m, precision, sl ? 1 : 0, dl, sl ? m->io_t.as<double>() : nullptr,
@@ -528,10 +528,29 @@ int eb_apply_sl_p1(eb_mesh mesh, int precision, const double* t, double* v)
   return set_error(EB_ERR_STATE, "eb_apply_sl_p1 is not available in this build yet");
 }
 
+int eb_apply_hypersingular_device(eb_mesh mesh, int precision, const double* d_u, double* d_q, void* stream)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  EB_CUDA(cudaSetDevice(mesh->m->device));
+  return eb::mesh_apply_hypersingular(mesh->m, precision, d_u, d_q, (cudaStream_t)stream);
+}
+
 int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double* q)
 {
-  (void)mesh; (void)precision; (void)u; (void)q;
-  return set_error(EB_ERR_STATE, "eb_apply_hypersingular is not available in this build yet");
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  if (!u || !q) return set_error(EB_ERR_INVALID, "null vector");
+  std::lock_guard<std::mutex> g(mesh->lock);
+  eb::Mesh* m = mesh->m;
+  EB_CUDA(cudaSetDevice(m->device));
+  const int nv = m->h.nv;
+  cudaStream_t st = mesh->stream;
+  EB_CHECK(m->io_u.alloc(sizeof(double) * nv));
+  EB_CHECK(m->io_q.alloc(sizeof(double) * std::max(nv, m->h.ne)));
+  EB_CUDA(cudaMemcpyAsync(m->io_u.p, u, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+  EB_CHECK(eb::mesh_apply_hypersingular(m, precision, m->io_u.as<double>(), m->io_q.as<double>(), st));
+  EB_CUDA(cudaMemcpyAsync(q, m->io_q.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+  EB_CUDA(cudaStreamSynchronize(st));
+  return EB_OK;
 }
 
 }  // extern "C"

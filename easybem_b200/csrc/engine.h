@@ -60,6 +60,8 @@ struct Mesh {
   // per-apply scratch
   DevBuf rec, partial, counter, items;
   DevBuf io_t, io_u, io_v, io_q;
+  // hypersingular: curl coefficients, vertex -> (triangle, local) lists, work vectors
+  DevBuf curl9, vtri_ptr, vtri_list, elems0, hs_x, hs_w;
   int nitems_work = 0;
   FarPlan plan;
   // one immutable device descriptor and launch shape per far-field variant
@@ -83,5 +85,8 @@ int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int orde
 // Device-pointer apply: t has nsl columns (stride ne), v likewise; u/q for DL.
 int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
                double* d_q, cudaStream_t st);
+
+// q = D u (hypersingular, curl form); u and q have nnodes entries (device).
+int mesh_apply_hypersingular(Mesh* m, int precision, const double* d_u, double* d_q, cudaStream_t st);
 
 }  // namespace eb

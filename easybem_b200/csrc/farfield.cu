@@ -399,16 +399,8 @@ static int occupancy_t(size_t smem)
 #define EB_FAR_CASES(X)                                                                                  \
   X(1, 1) X(3, 3) X(4, 4) X(6, 6) X(7, 7) X(8, 0)
 
-#define EB_FAR_DISPATCH(FN, RET, ...)                                                                    \
-  {                                                                                                      \
-    switch (NSL * 2 + (DL ? 1 : 0)) {                                                                    \
-      case 1: return dispatch_k<T, 0, true>(__VA_ARGS__);                                                \
-      case 2: return dispatch_k<T, 1, false>(__VA_ARGS__);                                               \
-      case 3: return dispatch_k<T, 1, true>(__VA_ARGS__);                                                \
-      case 8: return dispatch_k<T, 4, false>(__VA_ARGS__);                                               \
-      default: return RET;                                                                               \
-    }                                                                                                    \
-  }
+// Operator variants compiled: (SL charges, DL).
+#define EB_VARIANTS(V) V(0, true) V(1, false) V(1, true) V(3, false) V(4, false)
 
 template <typename T, int NSL, bool DL>
 static cudaError_t dispatch_k(int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, size_t smem,
@@ -435,31 +427,30 @@ template <typename T>
 static cudaError_t far_launch_t(int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
                                 int* dc, size_t smem, int grid, cudaStream_t st)
 {
-  switch (NSL * 2 + (DL ? 1 : 0)) {
-    case 1: return dispatch_k<T, 0, true>(K, Q, dm, di, n, dc, smem, grid, st);
-    case 2: return dispatch_k<T, 1, false>(K, Q, dm, di, n, dc, smem, grid, st);
-    case 3: return dispatch_k<T, 1, true>(K, Q, dm, di, n, dc, smem, grid, st);
-    case 8: return dispatch_k<T, 4, false>(K, Q, dm, di, n, dc, smem, grid, st);
-    default: return cudaErrorInvalidValue;
-  }
+#define V(NS, D) \
+  if (NSL == NS && DL == D) return dispatch_k<T, NS, D>(K, Q, dm, di, n, dc, smem, grid, st);
+  EB_VARIANTS(V)
+#undef V
+  return cudaErrorInvalidValue;
 }
 
 template <typename T>
 static int far_occ_t(int NSL, bool DL, int K, int Q, size_t smem)
 {
-  switch (NSL * 2 + (DL ? 1 : 0)) {
-    case 1: return dispatch_occ<T, 0, true>(K, Q, smem);
-    case 2: return dispatch_occ<T, 1, false>(K, Q, smem);
-    case 3: return dispatch_occ<T, 1, true>(K, Q, smem);
-    case 8: return dispatch_occ<T, 4, false>(K, Q, smem);
-    default: return 0;
-  }
+#define V(NS, D) \
+  if (NSL == NS && DL == D) return dispatch_occ<T, NS, D>(K, Q, smem);
+  EB_VARIANTS(V)
+#undef V
+  return 0;
 }
 
 bool far_variant_supported(int NSL, bool DL)
 {
-  const int code = NSL * 2 + (DL ? 1 : 0);
-  return code == 1 || code == 2 || code == 3 || code == 8;
+#define V(NS, D) \
+  if (NSL == NS && DL == D) return true;
+  EB_VARIANTS(V)
+#undef V
+  return false;
 }
 
 cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
@@ -485,13 +476,14 @@ static cudaError_t prep_launch_t(int NSL, bool DL, int ne, int Q, const void* po
   const int grid = (int)((n + blk - 1) / blk);
   const S* p = reinterpret_cast<const S*>(pos);
   S* r = reinterpret_cast<S*>(rec);
-  switch (NSL * 2 + (DL ? 1 : 0)) {
-    case 1: prep_kernel<T, 0, true><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
-    case 2: prep_kernel<T, 1, false><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
-    case 3: prep_kernel<T, 1, true><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
-    case 8: prep_kernel<T, 4, false><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r); break;
-    default: return cudaErrorInvalidValue;
+#define V(NS, D) \
+  if (NSL == NS && DL == D) {                                                                            \
+    prep_kernel<T, NS, D><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r);       \
+    return cudaGetLastError();                                                                           \
   }
+  EB_VARIANTS(V)
+#undef V
+  return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
@@ -514,15 +506,15 @@ cudaError_t finalize_launch(int NSL, bool DL, int ne, int nchunk, int nsplit, in
   finalize_kernel<NS, D><<<grid, blk, 0, st>>>(ne, nchunk, nsplit, nitems, iperm, trin, partial, sl_rowptr,     \
                                                sl_col, sl_val, dl_rowptr, dl_col, dl_val, t, tstride, u, v,    \
                                                vstride, q)
-  switch (NSL * 2 + (DL ? 1 : 0)) {
-    case 1: FIN(0, true); break;
-    case 2: FIN(1, false); break;
-    case 3: FIN(1, true); break;
-    case 8: FIN(4, false); break;
-    default: return cudaErrorInvalidValue;
+#define V(NS, D) \
+  if (NSL == NS && DL == D) {  \
+    FIN(NS, D);                \
+    return cudaGetLastError(); \
   }
+  EB_VARIANTS(V)
+#undef V
 #undef FIN
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace eb

@@ -88,6 +88,9 @@ int eb_apply_sl_p1(eb_mesh mesh, int precision, const double* t, double* v);
  * have nnodes entries. Replaces the empty applyGPULaplace3dHyperSing
  * (src/BEM3dLaplaceGPU.cu:1554-1555). */
 int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double* q);
+/* Device-pointer form of eb_apply_hypersingular on a stream (asynchronous). */
+int eb_apply_hypersingular_device(eb_mesh mesh, int precision, const double* d_u, double* d_q,
+                                  void* stream);
 
 /* The quadrature rules behind index `order` (host only, no GPU needed):
  * the Gauss-Legendre rule on [0,1] (up to 64 points) and the triangle rule on
