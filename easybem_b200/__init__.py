@@ -19,9 +19,9 @@ import os
 
 import numpy as np
 
-from ._lib import EB_PREC_FP64, EB_PREC_MIXED, EasyBemError, check, lib
+from ._lib import EB_PREC_FP64, EB_PREC_MIXED, EasyBemError, SolveOptions, SolveStats, check, lib
 
-__all__ = ["Mesh", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
+__all__ = ["Mesh", "Solver", "solve", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
            "apply_gpu_laplace3d_1layer_linears", "apply_gpu_laplace3d_2layer",
            "apply_gpu_laplace3d_hypersing", "version", "precision_code"]
 
@@ -136,6 +136,15 @@ class Mesh:
                                           ctypes.c_void_p(d_u or None), ctypes.c_void_p(d_v or None),
                                           ctypes.c_void_p(d_q or None), ctypes.c_void_p(stream or None)))
 
+    def dirichlet_rhs(self, g):
+        """b = (1/2) M g + K g for vertex data g ([nnodes] or [nrhs, nnodes]), FP64."""
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        one = g.ndim == 1
+        g2 = g.reshape(-1, self.nnodes)
+        b = np.empty((g2.shape[0], self.nelems))
+        check(lib().eb_dirichlet_rhs(self._h, g2.shape[0], _ptr(g2), _ptr(b)))
+        return b[0] if one else b
+
     def set_profiling(self, on: bool = True):
         check(lib().eb_set_profiling(self._h, 1 if on else 0))
 
@@ -143,6 +152,88 @@ class Mesh:
         a, b = ctypes.c_double(), ctypes.c_double()
         check(lib().eb_last_kernel_ms(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+
+class Solver:
+    """Batched GMRES with iterative refinement for V x = b (see include/easybem_gpu.h).
+
+    Systems (mesh, right-hand side) join with ``add`` and advance together with
+    ``step``; ``result`` returns (x, stats) once ``done``.
+    """
+
+    def __init__(self, tol=1e-8, inner_tol=1e-6, restart=50, max_cycles=40, max_iterations=4000,
+                 inner_precision="mixed"):
+        o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision))
+        h = ctypes.c_void_p()
+        check(lib().eb_solver_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._ne = {}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().eb_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, mesh: "Mesh", b):
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, mesh.nelems)
+        ids = (ctypes.c_int * b.shape[0])()
+        check(lib().eb_solver_add(self._h, mesh.handle, b.shape[0], _ptr(b), ids))
+        for i in ids:
+            self._ne[i] = mesh.nelems
+        return list(ids)
+
+    def step(self) -> int:
+        n = ctypes.c_int()
+        check(lib().eb_solver_step(self._h, ctypes.byref(n)))
+        return n.value
+
+    def done(self, sid: int) -> bool:
+        d = ctypes.c_int()
+        check(lib().eb_solver_done(self._h, int(sid), ctypes.byref(d)))
+        return bool(d.value)
+
+    def result(self, sid: int):
+        x = np.empty(self._ne[sid])
+        st = SolveStats()
+        check(lib().eb_solver_result(self._h, int(sid), _ptr(x), ctypes.byref(st)))
+        return x, {"converged": bool(st.converged), "cycles": st.cycles, "iterations": st.iterations,
+                   "rel_residual": st.rel_residual}
+
+    def remove(self, sid: int):
+        check(lib().eb_solver_remove(self._h, int(sid)))
+        self._ne.pop(sid, None)
+
+    def bytes_per_system(self, mesh: "Mesh") -> int:
+        n = ctypes.c_longlong()
+        check(lib().eb_solver_bytes_per_system(self._h, mesh.handle, ctypes.byref(n)))
+        return n.value
+
+
+def solve(problems, **options):
+    """Solves V x = b for a list of (mesh, b) with b [ne] or [nrhs, ne], all in lockstep.
+
+    Returns a list (per problem) of (x, stats) where x has b's shape and stats
+    is a list of per-right-hand-side dicts.
+    """
+    s = Solver(**options)
+    try:
+        ids = [s.add(m, b) for m, b in problems]
+        while s.step() > 0:
+            pass
+        out = []
+        for (m, b), idl in zip(problems, ids):
+            res = [s.result(i) for i in idl]
+            x = np.stack([r[0] for r in res])
+            out.append((x.reshape(np.shape(b)), [r[1] for r in res]))
+        return out
+    finally:
+        s.close()
 
 
 # ---------------------------------------------------------------------------

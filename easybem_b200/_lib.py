@@ -48,8 +48,29 @@ _SIGNATURES = {
                                      ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]),
     "eb_measure_fp32_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "eb_set_profiling": (ctypes.c_int, [_dp, ctypes.c_int]),
+    "eb_dirichlet_rhs": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_solve_options_default": (None, [_dp]),
+    "eb_solve_sl": (ctypes.c_int, [ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "eb_solver_create": (ctypes.c_int, [_dp, ctypes.POINTER(_dp)]),
+    "eb_solver_destroy": (ctypes.c_int, [_dp]),
+    "eb_solver_add": (ctypes.c_int, [_dp, _dp, ctypes.c_int, _dp, _dp]),
+    "eb_solver_step": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int)]),
+    "eb_solver_done": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "eb_solver_result": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_solver_remove": (ctypes.c_int, [_dp, ctypes.c_int]),
+    "eb_solver_bytes_per_system": (ctypes.c_int, [_dp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     "eb_last_kernel_ms": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
 }
+
+
+class SolveOptions(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("inner_tol", ctypes.c_double), ("restart", ctypes.c_int),
+                ("max_cycles", ctypes.c_int), ("max_iterations", ctypes.c_int), ("inner_precision", ctypes.c_int)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("converged", ctypes.c_int), ("cycles", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("rel_residual", ctypes.c_double)]
 
 
 class EasyBemError(RuntimeError):

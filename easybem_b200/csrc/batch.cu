@@ -1,0 +1,136 @@
+#include "batch.h"
+
+#include <algorithm>
+#include <numeric>
+#include <string>
+
+namespace eb {
+
+int batch_entry_init(BatchEntry* e, Mesh* m)
+{
+  const HostMesh& h = m->h;
+  e->mesh = m;
+  EB_CHECK(e->rec.alloc((size_t)h.ne * h.Q * rec_slots(kBatchCols, false) * sizeof(dq)));
+  EB_CHECK(e->partial.alloc(sizeof(double) * (size_t)kBatchCols * m->plan.nsplit * h.nitems));
+  EB_CHECK(e->tin.alloc(sizeof(double) * (size_t)kBatchCols * h.ne));
+  EB_CHECK(e->vout.alloc(sizeof(double) * (size_t)kBatchCols * h.ne));
+  EB_CUDA(cudaMemset(e->tin.p, 0, e->tin.bytes));
+  return EB_OK;
+}
+
+void Batch::reset_graph()
+{
+  if (exec_) cudaGraphExecDestroy(exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  exec_ = nullptr;
+  graph_ = nullptr;
+}
+
+int batch_width(int cols) { return cols <= 1 ? 1 : (cols <= 3 ? 3 : 4); }
+
+int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags)
+{
+  reset_graph();
+  entries_ = entries;
+  fp32_ = fp32;
+  nsl_ = batch_width(nsl);
+  nitems_ = grid_ = prep_blocks_ = fin_blocks_ = 0;
+  quad_pairs_ = 0;
+  if (entries.empty()) return EB_OK;
+  Q_ = entries[0]->mesh->h.Q;
+  K_ = entries[0]->mesh->h.K;
+  const int n = (int)entries.size();
+  std::vector<FarMeshDesc> desc(n);
+  std::vector<ApplyArgs> args(n);
+  std::vector<int> poff(n + 1, 0), foff(n + 1, 0);
+  std::vector<std::pair<long long, WorkItem>> items;
+  int src_tile = kTS;
+  for (int e = 0; e < n; e++) {
+    BatchEntry* be = entries[e];
+    be->index = e;
+    Mesh* m = be->mesh;
+    const HostMesh& h = m->h;
+    if (h.Q != Q_) return set_error(EB_ERR_INVALID, "a batch needs one quadrature order for all meshes");
+    desc[e] = mesh_far_desc(m, fp32, nsl_, false, be->rec.p, be->partial.as<double>());
+    desc[e].active = d_flags ? d_flags + e : nullptr;
+    src_tile = std::min(src_tile, desc[e].src_tile);
+    args[e] = mesh_apply_args(m, fp32, be->rec.p, be->partial.as<double>(), be->tin.as<double>(), h.ne, nullptr,
+                              be->vout.as<double>(), h.ne, nullptr);
+    args[e].active = d_flags ? d_flags + e : nullptr;
+    poff[e + 1] = poff[e] + (int)(((long long)h.ne * h.Q + kPrepBlock - 1) / kPrepBlock);
+    foff[e + 1] = foff[e] + (h.ne + kFinalizeBlock - 1) / kFinalizeBlock;
+    quad_pairs_ += h.far_quad_pairs;
+    for (WorkItem w : m->items_host) {
+      w.mesh = e;
+      const long long tg = std::min(kTT, h.nitems - w.tgt0);
+      const long long src = (long long)std::min(h.ne, w.cell1 * kCell) - (long long)w.cell0 * kCell;
+      items.push_back({tg * src, w});
+    }
+  }
+  for (auto& d : desc) d.src_tile = src_tile;
+  // longest items first: the dynamic queue then ends with the short ones
+  std::stable_sort(items.begin(), items.end(),
+                   [](const std::pair<long long, WorkItem>& a, const std::pair<long long, WorkItem>& b) {
+                     return a.first > b.first;
+                   });
+  std::vector<WorkItem> flat(items.size());
+  for (size_t k = 0; k < items.size(); k++) flat[k] = items[k].second;
+  nitems_ = (int)flat.size();
+  prep_blocks_ = poff[n];
+  fin_blocks_ = foff[n];
+
+  EB_CHECK(desc_.alloc(sizeof(FarMeshDesc) * n));
+  EB_CUDA(cudaMemcpy(desc_.p, desc.data(), sizeof(FarMeshDesc) * n, cudaMemcpyHostToDevice));
+  EB_CHECK(args_.alloc(sizeof(ApplyArgs) * n));
+  EB_CUDA(cudaMemcpy(args_.p, args.data(), sizeof(ApplyArgs) * n, cudaMemcpyHostToDevice));
+  EB_CHECK(items_.alloc(sizeof(WorkItem) * flat.size()));
+  EB_CUDA(cudaMemcpy(items_.p, flat.data(), sizeof(WorkItem) * flat.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(prep_off_.alloc(sizeof(int) * (n + 1)));
+  EB_CUDA(cudaMemcpy(prep_off_.p, poff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  EB_CHECK(fin_off_.alloc(sizeof(int) * (n + 1)));
+  EB_CUDA(cudaMemcpy(fin_off_.p, foff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  EB_CHECK(counter_.alloc(sizeof(int)));
+
+  smem_ = (size_t)src_tile * Q_ * rec_slots(nsl_, false) * (fp32 ? sizeof(float4) : sizeof(dq));
+  int occ = far_occupancy(fp32, nsl_, false, K_, Q_, smem_);
+  if (occ < 1) occ = 1;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  grid_ = std::min(nsm * occ, std::max(1, nitems_));
+  return EB_OK;
+}
+
+int Batch::run(cudaStream_t st)
+{
+  if (entries_.empty()) return EB_OK;
+  const int n = (int)entries_.size();
+  EB_CUDA(prep_launch_batch(fp32_, nsl_, false, args_.as<ApplyArgs>(), prep_off_.as<int>(), n, prep_blocks_, st));
+  EB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(int), st));
+  EB_CUDA(far_launch(fp32_, nsl_, false, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
+                     counter_.as<int>(), smem_, grid_, st));
+  EB_CUDA(finalize_launch_batch(nsl_, false, args_.as<ApplyArgs>(), fin_off_.as<int>(), n, fin_blocks_, st));
+  return EB_OK;
+}
+
+int Batch::run_graph(cudaStream_t st)
+{
+  if (entries_.empty()) return EB_OK;
+  if (!exec_) {
+    EB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = run(st);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != EB_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    EB_CUDA(e);
+    graph_ = g;
+    EB_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+  }
+  EB_CUDA(cudaGraphLaunch(exec_, st));
+  return EB_OK;
+}
+
+}  // namespace eb

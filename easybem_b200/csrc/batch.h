@@ -1,0 +1,66 @@
+// Batched apply: the far field of many meshes and right-hand sides in one
+// persistent launch.
+//
+// Not in the reference, whose GPU path holds a single process-global mesh
+// (src/meshTopology.cpp:11-19). An entry is one mesh with up to kBatchCols
+// SL right-hand sides (and optionally one DL density); it owns its apply
+// scratch and its input/output columns. A Batch merges the work items of all
+// entries (largest first, pulled dynamically by the persistent CTAs), so one
+// apply over any number of uneven meshes is four launches: batched record
+// preparation, a counter reset, the far-field kernel and a batched finalize
+// (near field included). Entries can be switched off per apply through a
+// device flag without rebuilding the batch, and a built batch can be
+// captured once into a CUDA graph and replayed.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "engine.h"
+
+namespace eb {
+
+constexpr int kBatchCols = 4;  // SL right-hand sides per entry (the NSL = 4 far-field variant)
+
+struct BatchEntry {
+  Mesh* mesh = nullptr;
+  DevBuf rec, partial;  // apply scratch
+  DevBuf tin, vout;     // kBatchCols columns of nelems each (inputs / outputs)
+  int index = -1;       // position in the current batch
+};
+
+class Batch {
+ public:
+  // Builds the launch tables for `entries` (all meshes must share the
+  // quadrature order). fp32 selects the mixed-precision far field.
+  // nsl: right-hand sides computed per entry (1, 3 or 4; columns beyond an
+  // entry's systems carry zeros).
+  int build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags);
+  // One apply of all entries whose flag is set (inputs tin, outputs vout).
+  int run(cudaStream_t st);
+  // Captures run() into a CUDA graph on first use and replays it afterwards.
+  int run_graph(cudaStream_t st);
+  void reset_graph();
+  ~Batch() { reset_graph(); }
+
+  int nentries() const { return (int)entries_.size(); }
+  long long quad_pairs() const { return quad_pairs_; }
+
+ private:
+  std::vector<BatchEntry*> entries_;
+  bool fp32_ = true;
+  int nsl_ = kBatchCols;
+  DevBuf desc_, items_, args_, prep_off_, fin_off_, counter_;
+  int nitems_ = 0, grid_ = 0, prep_blocks_ = 0, fin_blocks_ = 0, K_ = 0, Q_ = 0;
+  size_t smem_ = 0;
+  long long quad_pairs_ = 0;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+};
+
+// Far-field variant width (SL charges) for entries using up to `cols` columns.
+int batch_width(int cols);
+// Allocates an entry's scratch and columns for mesh m.
+int batch_entry_init(BatchEntry* e, Mesh* m);
+
+}  // namespace eb

@@ -238,7 +238,7 @@ static size_t slot_bytes(bool fp32) { return fp32 ? sizeof(float4) : sizeof(dq);
 
 // Source triangles per shared-memory tile for a variant (whole cells when
 // they fit; large quadrature rules fall back to smaller tiles).
-static int src_tile_for(int Q, bool fp32, int nsl, bool dl)
+int src_tile_for(int Q, bool fp32, int nsl, bool dl)
 {
   const size_t per_tri = (size_t)Q * rec_slots(nsl, dl) * slot_bytes(fp32);
   const size_t budget = 40 * 1024;
@@ -263,6 +263,7 @@ static int build_items(Mesh* m)
       items.push_back(WorkItem{0, t * kTT, sp * cells_per, std::min(h.ncells, (sp + 1) * cells_per), sp});
   m->plan.nsplit = nsplit;
   m->nitems_work = (int)items.size();
+  m->items_host = items;
   EB_CHECK(upload(m->items, items));
   EB_CHECK(m->counter.alloc(sizeof(int)));
   return EB_OK;
@@ -288,6 +289,67 @@ int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int orde
   return EB_OK;
 }
 
+ApplyArgs mesh_apply_args(const Mesh* m, bool fp32, void* rec, const double* partial, const double* t, int tstride,
+                          const double* u, double* v, int vstride, double* q)
+{
+  const HostMesh& h = m->h;
+  ApplyArgs A;
+  A.pos = fp32 ? m->pos32.p : m->pos64.p;
+  A.wj = m->wj.as<double>();
+  A.svid = m->svid.as<int4>();
+  A.perm = m->perm.as<int>();
+  A.bary = m->bary.as<double>();
+  A.t = t;
+  A.tstride = tstride;
+  A.u = u;
+  A.rec = rec;
+  A.ne = h.ne;
+  A.Q = h.Q;
+  A.nchunk = h.nchunk;
+  A.nsplit = m->plan.nsplit;
+  A.nitems = h.nitems;
+  A.iperm = m->iperm.as<int>();
+  A.trin = m->trin.as<dq>();
+  A.partial = partial;
+  A.sl_rowptr = m->sl_rowptr.as<int>();
+  A.sl_col = m->sl_col.as<int>();
+  A.sl_val = m->sl_val.as<double>();
+  A.dl_rowptr = m->dl_rowptr.as<int>();
+  A.dl_col = m->dl_col.as<int>();
+  A.dl_val = m->dl_val.as<double>();
+  A.v = v;
+  A.vstride = vstride;
+  A.q = q;
+  A.active = nullptr;
+  return A;
+}
+
+FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec, double* partial)
+{
+  const HostMesh& h = m->h;
+  FarMeshDesc desc;
+  desc.tgt32 = m->tgt32.as<float4>();
+  desc.tgt64 = m->tgt64.as<dq>();
+  desc.tcent = m->tcent.as<dq>();
+  desc.tnrm = m->tnrm.as<dq>();
+  desc.snrm = m->snrm.as<dq>();
+  desc.splane32 = m->splane32.as<float4>();
+  desc.splane64 = m->splane64.as<dq>();
+  desc.tvid = m->tvid.as<int4>();
+  desc.rec = rec;
+  desc.svid = m->svid.as<int4>();
+  desc.ccent = m->ccent.as<dq>();
+  desc.ttile = m->ttile.as<dq>();
+  desc.partial = partial;
+  desc.nitems = h.nitems;
+  desc.ne = h.ne;
+  desc.Q = h.Q;
+  desc.nsplit = m->plan.nsplit;
+  desc.src_tile = src_tile_for(h.Q, fp32, nsl, dl);
+  desc.active = nullptr;
+  return desc;
+}
+
 int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
                double* d_q, cudaStream_t st)
 {
@@ -307,25 +369,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
   }
   Mesh::Variant& var = m->variants[(fp32 ? 64 : 0) + nsl * 2 + (dl ? 1 : 0)];
   if (!var.desc.p) {
-    FarMeshDesc desc;
-    desc.tgt32 = m->tgt32.as<float4>();
-    desc.tgt64 = m->tgt64.as<dq>();
-    desc.tcent = m->tcent.as<dq>();
-    desc.tnrm = m->tnrm.as<dq>();
-    desc.snrm = m->snrm.as<dq>();
-    desc.tvid = m->tvid.as<int4>();
-    desc.rec = m->rec.p;
-    desc.svid = m->svid.as<int4>();
-    desc.ccent = m->ccent.as<dq>();
-    desc.ttile = m->ttile.as<dq>();
-    desc.splane32 = m->splane32.as<float4>();
-    desc.splane64 = m->splane64.as<dq>();
-    desc.partial = m->partial.as<double>();
-    desc.nitems = h.nitems;
-    desc.ne = h.ne;
-    desc.Q = h.Q;
-    desc.nsplit = m->plan.nsplit;
-    desc.src_tile = src_tile_for(h.Q, fp32, nsl, dl);
+    const FarMeshDesc desc = mesh_far_desc(m, fp32, nsl, dl, m->rec.p, m->partial.as<double>());
     const size_t smem = (size_t)desc.src_tile * h.Q * nrec * sb;
     int occ = far_occupancy(fp32, nsl, dl, h.K, h.Q, smem);
     if (occ < 1) occ = 1;
@@ -337,9 +381,8 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
     var.smem = smem;
     var.src_tile = desc.src_tile;
   }
-  const void* pos = fp32 ? m->pos32.p : m->pos64.p;
-  EB_CUDA(prep_launch(fp32, nsl, dl, h.ne, h.Q, pos, m->wj.as<double>(), m->svid.as<int4>(), m->perm.as<int>(),
-                      m->bary.as<double>(), d_t, h.ne, d_u, m->rec.p, st));
+  const ApplyArgs A = mesh_apply_args(m, fp32, m->rec.p, m->partial.as<double>(), d_t, h.ne, d_u, d_v, h.ne, d_q);
+  EB_CUDA(prep_launch(fp32, nsl, dl, A, st));
   EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
   if (m->profile) {
     if (!m->ev0) {
@@ -355,10 +398,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
   m->plan.smem = var.smem;
   m->plan.src_tile = var.src_tile;
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev1, st));
-  EB_CUDA(finalize_launch(nsl, dl, h.ne, h.nchunk, m->plan.nsplit, h.nitems, m->iperm.as<int>(), m->trin.as<dq>(),
-                          m->partial.as<double>(), m->sl_rowptr.as<int>(), m->sl_col.as<int>(),
-                          m->sl_val.as<double>(), m->dl_rowptr.as<int>(), m->dl_col.as<int>(),
-                          m->dl_val.as<double>(), d_t, h.ne, d_u, d_v, h.ne, d_q, st));
+  EB_CUDA(finalize_launch(nsl, dl, A, st));
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev2, st));
   return EB_OK;
 }
@@ -480,6 +520,28 @@ int eb_apply_sl_dl(eb_mesh mesh, int precision, const double* t, const double* u
 {
   if (!t || !u || !v || !q) return set_error(EB_ERR_INVALID, "null vector");
   return host_apply(mesh, precision, t, u, v, q);
+}
+
+int eb_dirichlet_rhs(eb_mesh mesh, int nrhs, const double* g, double* b)
+{
+  if (!mesh || !g || !b || nrhs < 1) return set_error(EB_ERR_INVALID, "null argument");
+  const eb::HostMesh& h = mesh->m->h;
+  for (int c = 0; c < nrhs; c++) {
+    const double* gc = g + (size_t)c * h.nv;
+    double* bc = b + (size_t)c * h.ne;
+    EB_CHECK(eb_apply_dl_p1(mesh, EB_PREC_FP64, gc, bc));
+    // + (1/2) M g with M[i][node] = J_i / 6 (src/BEM3dLaplace.cpp:469-477)
+    for (int i = 0; i < h.ne; i++) {
+      const int* f = &h.elems[3 * i];
+      const eb::d3 p0 = eb::mk3(h.nodes[3 * f[0]], h.nodes[3 * f[0] + 1], h.nodes[3 * f[0] + 2]);
+      const eb::d3 p1 = eb::mk3(h.nodes[3 * f[1]], h.nodes[3 * f[1] + 1], h.nodes[3 * f[1] + 2]);
+      const eb::d3 p2 = eb::mk3(h.nodes[3 * f[2]], h.nodes[3 * f[2] + 1], h.nodes[3 * f[2] + 2]);
+      const eb::d3 n = eb::cross3(p1 - p0, p2 - p0);
+      const double J = std::sqrt(eb::dot3(n, n));
+      bc[i] += 0.5 * (J / 6.0) * (gc[f[0]] + gc[f[1]] + gc[f[2]]);
+    }
+  }
+  return EB_OK;
 }
 
 int eb_quadrature(int order, int* nline, double* lx, double* lw, int* ntri, double* tx, double* ty, double* tw)

@@ -14,14 +14,12 @@ cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshD
                        int* dc, size_t smem, int grid, cudaStream_t st);
 int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem);
 bool far_variant_supported(int NSL, bool DL);
-cudaError_t prep_launch(bool fp32, int NSL, bool DL, int ne, int Q, const void* pos, const double* wj,
-                        const int4* svid, const int* perm, const double* bary, const double* t, int tstride,
-                        const double* u, void* rec, cudaStream_t st);
-cudaError_t finalize_launch(int NSL, bool DL, int ne, int nchunk, int nsplit, int nitems, const int* iperm,
-                            const dq* trin, const double* partial, const int* sl_rowptr, const int* sl_col,
-                            const double* sl_val, const int* dl_rowptr, const int* dl_col, const double* dl_val,
-                            const double* t, int tstride, const double* u, double* v, int vstride, double* q,
-                            cudaStream_t st);
+cudaError_t prep_launch(bool fp32, int NSL, bool DL, const ApplyArgs& A, cudaStream_t st);
+cudaError_t finalize_launch(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st);
+cudaError_t prep_launch_batch(bool fp32, int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n,
+                              int nblocks, cudaStream_t st);
+cudaError_t finalize_launch_batch(int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
+                                  cudaStream_t st);
 
 // Simple owning device buffer.
 struct DevBuf {
@@ -59,6 +57,7 @@ struct Mesh {
   long long npairs = 0;
   // per-apply scratch
   DevBuf rec, partial, counter, items;
+  std::vector<WorkItem> items_host;
   DevBuf io_t, io_u, io_v, io_q;
   // hypersingular: curl coefficients, vertex -> (triangle, local) lists, work vectors
   DevBuf curl9, vtri_ptr, vtri_list, elems0, hs_x, hs_w;
@@ -82,6 +81,13 @@ struct Mesh {
 };
 
 int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int order, Mesh** out);
+// Prep/finalize arguments of mesh m for the given scratch and vectors.
+ApplyArgs mesh_apply_args(const Mesh* m, bool fp32, void* rec, const double* partial, const double* t, int tstride,
+                          const double* u, double* v, int vstride, double* q);
+// Source triangles per shared-memory tile of a far-field variant.
+int src_tile_for(int Q, bool fp32, int nsl, bool dl);
+// Far-field descriptor of mesh m for the given scratch.
+FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec, double* partial);
 // Device-pointer apply: t has nsl columns (stride ne), v likewise; u/q for DL.
 int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
                double* d_q, cudaStream_t st);

@@ -183,6 +183,7 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
     if (it >= nitems) break;
     const WorkItem w = items[it];
     const FarMeshDesc md = meshes[w.mesh];
+    if (md.active && *md.active == 0) continue;  // uniform across the CTA
     const int nq = md.Q;
     const int ti = w.tgt0 + threadIdx.x;
     const bool active = ti < md.nitems;
@@ -298,32 +299,28 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
 // Source records for one apply: positions (static) with the per-apply
 // strengths s = w_b J_j u_h(y_b) (DL) and charges c_r = w_b J_j t_r[j] (SL).
 template <typename T, int NSL, bool DL>
-__global__ void prep_kernel(int ne, int Q, const typename Slot<T>::type* __restrict__ pos,
-                            const double* __restrict__ wj_tab, const int4* __restrict__ svid,
-                            const int* __restrict__ perm, const double* __restrict__ bary,
-                            const double* __restrict__ t, int tstride, const double* __restrict__ u,
-                            typename Slot<T>::type* __restrict__ rec)
+__device__ __forceinline__ void prep_point(const ApplyArgs& A, long long idx)
 {
   using S = typename Slot<T>::type;
   constexpr int NREC = rec_slots(NSL, DL);
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)ne * Q) return;
-  const int j = (int)(idx / Q), b = (int)(idx % Q);
-  const double wj = wj_tab[idx];  // w_b * J_j
-  const int orig = perm[j];
+  if (idx >= (long long)A.ne * A.Q || (A.active && *A.active == 0)) return;
+  const int j = (int)(idx / A.Q), b = (int)(idx % A.Q);
+  const double wj = A.wj[idx];  // w_b * J_j
+  const int orig = A.perm[j];
   T vals[4 * NREC];
 #pragma unroll
   for (int k = 0; k < 4 * NREC; ++k) vals[k] = 0;
 #pragma unroll
-  for (int c = 0; c < NSL; ++c) vals[4 * charge_slot(c, DL) + charge_comp(c, DL)] = (T)(wj * t[(size_t)c * tstride + orig]);
+  for (int c = 0; c < NSL; ++c)
+    vals[4 * charge_slot(c, DL) + charge_comp(c, DL)] = (T)(wj * A.t[(size_t)c * A.tstride + orig]);
   if constexpr (DL) {
-    const int4 v = svid[j];
-    const double e1 = bary[2 * b], e2 = bary[2 * b + 1];
-    const double uh = (1.0 - e1 - e2) * u[v.x] + e1 * u[v.y] + e2 * u[v.z];
+    const int4 v = A.svid[j];
+    const double e1 = A.bary[2 * b], e2 = A.bary[2 * b + 1];
+    const double uh = (1.0 - e1 - e2) * A.u[v.x] + e1 * A.u[v.y] + e2 * A.u[v.z];
     vals[4] = (T)(wj * uh);
   }
-  S* r = rec + idx * NREC;
-  r[0] = pos[idx];
+  S* r = reinterpret_cast<S*>(A.rec) + idx * NREC;
+  r[0] = reinterpret_cast<const S*>(A.pos)[idx];
 #pragma unroll
   for (int k = 1; k < NREC; ++k) {
     S o;
@@ -332,38 +329,71 @@ __global__ void prep_kernel(int ne, int Q, const typename Slot<T>::type* __restr
   }
 }
 
-// Output rows in original order: sum the partial slots of the triangle's
+// Output row i (original order): sum the partial slots of the triangle's
 // items in a fixed order, scale by J_i / (4 pi) and add the FP64 near field.
 template <int NSL, bool DL>
-__global__ void finalize_kernel(int ne, int nchunk, int nsplit, int nitems, const int* __restrict__ iperm,
-                                const dq* __restrict__ trin, const double* __restrict__ partial,
-                                const int* __restrict__ sl_rowptr, const int* __restrict__ sl_col,
-                                const double* __restrict__ sl_val, const int* __restrict__ dl_rowptr,
-                                const int* __restrict__ dl_col, const double* __restrict__ dl_val,
-                                const double* __restrict__ t, int tstride, const double* __restrict__ u,
-                                double* __restrict__ v, int vstride, double* __restrict__ q)
+__device__ __forceinline__ void finalize_row(const ApplyArgs& A, int i)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ne) return;
-  const int s = iperm[i];
-  const double scale = trin[s].w * (0.25 / M_PI);
-  const size_t stride = (size_t)nsplit * nitems;
+  if (i >= A.ne || (A.active && *A.active == 0)) return;
+  const int s = A.iperm[i];
+  const double scale = A.trin[s].w * (0.25 / M_PI);
+  const size_t stride = (size_t)A.nsplit * A.nitems;
   for (int c = 0; c < NSL; ++c) {
     double far = 0.0;
-    for (int sp = 0; sp < nsplit; ++sp)
-      for (int ch = 0; ch < nchunk; ++ch) far += partial[c * stride + (size_t)sp * nitems + (size_t)s * nchunk + ch];
+    for (int sp = 0; sp < A.nsplit; ++sp)
+      for (int ch = 0; ch < A.nchunk; ++ch)
+        far += A.partial[c * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
     double nr = 0.0;
-    for (int k = sl_rowptr[i]; k < sl_rowptr[i + 1]; ++k) nr += sl_val[k] * t[(size_t)c * tstride + sl_col[k]];
-    v[(size_t)c * vstride + i] = scale * far + nr;
+    for (int k = A.sl_rowptr[i]; k < A.sl_rowptr[i + 1]; ++k) nr += A.sl_val[k] * A.t[(size_t)c * A.tstride + A.sl_col[k]];
+    A.v[(size_t)c * A.vstride + i] = scale * far + nr;
   }
   if (DL) {
     double far = 0.0;
-    for (int sp = 0; sp < nsplit; ++sp)
-      for (int ch = 0; ch < nchunk; ++ch) far += partial[NSL * stride + (size_t)sp * nitems + (size_t)s * nchunk + ch];
+    for (int sp = 0; sp < A.nsplit; ++sp)
+      for (int ch = 0; ch < A.nchunk; ++ch)
+        far += A.partial[NSL * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
     double nr = 0.0;
-    for (int k = dl_rowptr[i]; k < dl_rowptr[i + 1]; ++k) nr += dl_val[k] * u[dl_col[k]];
-    q[i] = scale * far + nr;
+    for (int k = A.dl_rowptr[i]; k < A.dl_rowptr[i + 1]; ++k) nr += A.dl_val[k] * A.u[A.dl_col[k]];
+    A.q[i] = scale * far + nr;
   }
+}
+
+template <typename T, int NSL, bool DL>
+__global__ void prep_kernel(ApplyArgs A)
+{
+  prep_point<T, NSL, DL>(A, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+template <int NSL, bool DL>
+__global__ void finalize_kernel(ApplyArgs A)
+{
+  finalize_row<NSL, DL>(A, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Batched forms: block b belongs to entry e with off[e] <= b < off[e+1].
+__device__ __forceinline__ int entry_of_block(const int* __restrict__ off, int n, int b)
+{
+  int lo = 0, hi = n;  // off[lo] <= b < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <typename T, int NSL, bool DL>
+__global__ void prep_batch_kernel(const ApplyArgs* __restrict__ args, const int* __restrict__ off, int n)
+{
+  const int e = entry_of_block(off, n, blockIdx.x);
+  prep_point<T, NSL, DL>(args[e], (long long)(blockIdx.x - off[e]) * blockDim.x + threadIdx.x);
+}
+
+template <int NSL, bool DL>
+__global__ void finalize_batch_kernel(const ApplyArgs* __restrict__ args, const int* __restrict__ off, int n)
+{
+  const int e = entry_of_block(off, n, blockIdx.x);
+  finalize_row<NSL, DL>(args[e], (blockIdx.x - off[e]) * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -466,54 +496,70 @@ int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem)
 }
 
 template <typename T>
-static cudaError_t prep_launch_t(int NSL, bool DL, int ne, int Q, const void* pos, const double* wj, const int4* svid,
-                                 const int* perm, const double* bary, const double* t, int tstride, const double* u,
-                                 void* rec, cudaStream_t st)
+static cudaError_t prep_launch_t(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st)
 {
-  using S = typename Slot<T>::type;
-  const long long n = (long long)ne * Q;
+  const long long n = (long long)A.ne * A.Q;
   const int blk = 256;
   const int grid = (int)((n + blk - 1) / blk);
-  const S* p = reinterpret_cast<const S*>(pos);
-  S* r = reinterpret_cast<S*>(rec);
-#define V(NS, D) \
-  if (NSL == NS && DL == D) {                                                                            \
-    prep_kernel<T, NS, D><<<grid, blk, 0, st>>>(ne, Q, p, wj, svid, perm, bary, t, tstride, u, r);       \
-    return cudaGetLastError();                                                                           \
+#define V(NS, D)                                                \
+  if (NSL == NS && DL == D) {                                   \
+    prep_kernel<T, NS, D><<<grid, blk, 0, st>>>(A);             \
+    return cudaGetLastError();                                  \
   }
   EB_VARIANTS(V)
 #undef V
   return cudaErrorInvalidValue;
-  return cudaGetLastError();
 }
 
-cudaError_t prep_launch(bool fp32, int NSL, bool DL, int ne, int Q, const void* pos, const double* wj,
-                        const int4* svid, const int* perm, const double* bary, const double* t, int tstride,
-                        const double* u, void* rec, cudaStream_t st)
+cudaError_t prep_launch(bool fp32, int NSL, bool DL, const ApplyArgs& A, cudaStream_t st)
 {
-  return fp32 ? prep_launch_t<float>(NSL, DL, ne, Q, pos, wj, svid, perm, bary, t, tstride, u, rec, st)
-              : prep_launch_t<double>(NSL, DL, ne, Q, pos, wj, svid, perm, bary, t, tstride, u, rec, st);
+  return fp32 ? prep_launch_t<float>(NSL, DL, A, st) : prep_launch_t<double>(NSL, DL, A, st);
 }
 
-cudaError_t finalize_launch(int NSL, bool DL, int ne, int nchunk, int nsplit, int nitems, const int* iperm,
-                            const dq* trin, const double* partial, const int* sl_rowptr, const int* sl_col,
-                            const double* sl_val, const int* dl_rowptr, const int* dl_col, const double* dl_val,
-                            const double* t, int tstride, const double* u, double* v, int vstride, double* q,
-                            cudaStream_t st)
+cudaError_t finalize_launch(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st)
 {
-  const int blk = 128, grid = (ne + blk - 1) / blk;
-#define FIN(NS, D)                                                                                              \
-  finalize_kernel<NS, D><<<grid, blk, 0, st>>>(ne, nchunk, nsplit, nitems, iperm, trin, partial, sl_rowptr,     \
-                                               sl_col, sl_val, dl_rowptr, dl_col, dl_val, t, tstride, u, v,    \
-                                               vstride, q)
-#define V(NS, D) \
-  if (NSL == NS && DL == D) {  \
-    FIN(NS, D);                \
-    return cudaGetLastError(); \
+  const int blk = 128, grid = (A.ne + blk - 1) / blk;
+#define V(NS, D)                                                \
+  if (NSL == NS && DL == D) {                                   \
+    finalize_kernel<NS, D><<<grid, blk, 0, st>>>(A);            \
+    return cudaGetLastError();                                  \
   }
   EB_VARIANTS(V)
 #undef V
-#undef FIN
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
+static cudaError_t prep_batch_t(int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
+                                cudaStream_t st)
+{
+#define V(NS, D)                                                                  \
+  if (NSL == NS && DL == D) {                                                     \
+    prep_batch_kernel<T, NS, D><<<nblocks, kPrepBlock, 0, st>>>(d_args, d_off, n); \
+    return cudaGetLastError();                                                    \
+  }
+  EB_VARIANTS(V)
+#undef V
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t prep_launch_batch(bool fp32, int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n,
+                              int nblocks, cudaStream_t st)
+{
+  return fp32 ? prep_batch_t<float>(NSL, DL, d_args, d_off, n, nblocks, st)
+              : prep_batch_t<double>(NSL, DL, d_args, d_off, n, nblocks, st);
+}
+
+cudaError_t finalize_launch_batch(int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
+                                  cudaStream_t st)
+{
+#define V(NS, D)                                                                          \
+  if (NSL == NS && DL == D) {                                                             \
+    finalize_batch_kernel<NS, D><<<nblocks, kFinalizeBlock, 0, st>>>(d_args, d_off, n);   \
+    return cudaGetLastError();                                                            \
+  }
+  EB_VARIANTS(V)
+#undef V
   return cudaErrorInvalidValue;
 }
 

@@ -34,6 +34,8 @@ constexpr int kTT = 128;  // target items (threads) per CTA
 constexpr int kTS = 64;   // source triangles per shared-memory tile (Q <= 7)
 constexpr int kMaxRecSlots = 3;  // record slots of the widest variant
 constexpr int kMaxOutputs = 5;   // SL charges + DL of the widest variant
+constexpr int kPrepBlock = 256;     // threads per block of the record preparation (one source point each)
+constexpr int kFinalizeBlock = 128; // threads per block of the finalize (one output row each)
 
 // FP64 record slot (two 16-byte halves).
 struct __align__(16) dq {
@@ -73,11 +75,43 @@ struct FarMeshDesc {
   const dq* ccent;      // [ncells]: cell centre and bounding radius (FP64)
   const dq* ttile;      // [ntiles]: target-tile centre and bounding radius (FP64)
   double* partial;      // [nout][nsplit][nitems]
+  const int* active;    // optional: skip this mesh's work while *active == 0
   int nitems, ne, Q, nsplit, src_tile;
 };
 
 struct WorkItem {
   int mesh, tgt0, cell0, cell1, split;
+};
+
+// Per-mesh arguments of the record-preparation and finalize kernels (device
+// pointers); a batch passes an array of them.
+struct ApplyArgs {
+  // source records
+  const void* pos;       // static positions (float4 or dq)
+  const double* wj;      // w_b J_j per source point
+  const int4* svid;      // sorted source triangle vertex ids
+  const int* perm;       // sorted -> original triangle index
+  const double* bary;    // triangle-rule points (eta1, eta2)
+  const double* t;       // SL densities, nsl columns of stride tstride
+  int tstride;
+  const double* u;       // DL density (vertex values)
+  void* rec;             // records out
+  int ne, Q;
+  // finalize
+  int nchunk, nsplit, nitems;
+  const int* iperm;
+  const dq* trin;        // per sorted triangle: unit normal, J
+  const double* partial;
+  const int* sl_rowptr;
+  const int* sl_col;
+  const double* sl_val;
+  const int* dl_rowptr;
+  const int* dl_col;
+  const double* dl_val;
+  double* v;             // SL outputs, nsl columns of stride vstride
+  int vstride;
+  double* q;             // DL output
+  const int* active;     // optional: skip this mesh while *active == 0
 };
 
 }  // namespace eb

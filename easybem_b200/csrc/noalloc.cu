@@ -94,26 +94,7 @@ extern "C" int eb_apply_sl_dl_noalloc(eb_mesh handle, int precision, const doubl
   double* partial = reinterpret_cast<double*>(base + off_part);
   cudaStream_t st = (cudaStream_t)stream;
 
-  FarMeshDesc desc;
-  desc.tgt32 = m->tgt32.as<float4>();
-  desc.tgt64 = m->tgt64.as<dq>();
-  desc.tcent = m->tcent.as<dq>();
-  desc.tnrm = m->tnrm.as<dq>();
-  desc.snrm = m->snrm.as<dq>();
-  desc.splane32 = m->splane32.as<float4>();
-  desc.splane64 = m->splane64.as<dq>();
-  desc.tvid = m->tvid.as<int4>();
-  desc.rec = rec;
-  desc.svid = m->svid.as<int4>();
-  desc.ccent = m->ccent.as<dq>();
-  desc.ttile = m->ttile.as<dq>();
-  desc.partial = partial;
-  desc.nitems = h.nitems;
-  desc.ne = h.ne;
-  desc.Q = h.Q;
-  desc.nsplit = m->plan.nsplit;
-  const size_t per_tri = (size_t)h.Q * nrec * slot;
-  desc.src_tile = (int)std::max<size_t>(1, std::min<size_t>(kTS, (40 * 1024) / per_tri));
+  const FarMeshDesc desc = mesh_far_desc(m, fp32, nsl, dl, rec, partial);
   const size_t smem = (size_t)desc.src_tile * h.Q * nrec * slot;
   int occ = far_occupancy(fp32, nsl, dl, h.K, h.Q, smem);
   if (occ < 1) occ = 1;
@@ -123,15 +104,11 @@ extern "C" int eb_apply_sl_dl_noalloc(eb_mesh handle, int precision, const doubl
 
   noalloc_store_desc<<<1, 32, 0, st>>>(desc, d_desc);
   EB_CUDA(cudaGetLastError());
-  const void* pos = fp32 ? m->pos32.p : m->pos64.p;
-  EB_CUDA(prep_launch(fp32, nsl, dl, h.ne, h.Q, pos, m->wj.as<double>(), m->svid.as<int4>(), m->perm.as<int>(),
-                      m->bary.as<double>(), d_t, h.ne, d_u, rec, st));
+  const ApplyArgs A = mesh_apply_args(m, fp32, rec, partial, d_t, h.ne, d_u, d_v, h.ne, d_q);
+  EB_CUDA(prep_launch(fp32, nsl, dl, A, st));
   EB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
   EB_CUDA(far_launch(fp32, nsl, dl, h.K, h.Q, d_desc, m->items.as<WorkItem>(), m->nitems_work, counter, smem, grid,
                      st));
-  EB_CUDA(finalize_launch(nsl, dl, h.ne, h.nchunk, m->plan.nsplit, h.nitems, m->iperm.as<int>(), m->trin.as<dq>(),
-                          partial, m->sl_rowptr.as<int>(), m->sl_col.as<int>(), m->sl_val.as<double>(),
-                          m->dl_rowptr.as<int>(), m->dl_col.as<int>(), m->dl_val.as<double>(), d_t, h.ne, d_u, d_v,
-                          h.ne, d_q, st));
+  EB_CUDA(finalize_launch(nsl, dl, A, st));
   return EB_OK;
 }

@@ -92,6 +92,61 @@ int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double*
 int eb_apply_hypersingular_device(eb_mesh mesh, int precision, const double* d_u, double* d_q,
                                   void* stream);
 
+/* ---- Solves: V x = b (P0 single layer) by GMRES with iterative refinement.
+ * No counterpart in the reference (its drivers call SciPy CG on FP32 GPU
+ * matvecs, python/examples/laplace3dDirichletGPU.py:64-81). Each restart
+ * cycle of GMRES(restart) uses the `inner_precision` apply (mixed: FP32 far
+ * field); the Arnoldi basis and Gram-Schmidt are FP64 on the GPU; every cycle
+ * ends with the FP64 residual b - V x, and a system stops when
+ * ||b - V x|| <= tol ||b||. Many systems (meshes x right-hand sides) advance in
+ * lockstep through batched applies. */
+typedef struct eb_solve_options {
+  double tol;          /* FP64 relative residual target (default 1e-8) */
+  double inner_tol;    /* relative reduction per GMRES cycle (default 1e-6) */
+  int restart;         /* Krylov dimension (default 50) */
+  int max_cycles;      /* refinement cycles per system (default 40) */
+  int max_iterations;  /* GMRES iterations per system (default 4000) */
+  int inner_precision; /* EB_PREC_MIXED (default) or EB_PREC_FP64 */
+} eb_solve_options;
+
+typedef struct eb_solve_stats {
+  int converged;
+  int cycles;
+  int iterations;
+  double rel_residual; /* final ||b - V x|| / ||b|| from the FP64 apply */
+} eb_solve_stats;
+
+void eb_solve_options_default(eb_solve_options* opt);
+/* Solves sum(nrhs) systems at once: b[i] and x[i] are host arrays
+ * [nrhs[i]][nelems of meshes[i]]; stats (optional) has one entry per system
+ * in mesh-major order. All meshes need the same quadrature order. Returns
+ * EB_ERR_NOT_CONVERGED if any system missed the tolerance (x still holds the
+ * last iterate). */
+int eb_solve_sl(int nmesh, const eb_mesh* meshes, const int* nrhs, const double* const* b, double* const* x,
+                const eb_solve_options* opt, eb_solve_stats* stats);
+
+/* Stepwise form for continuous batching: systems join and leave between
+ * steps; one step advances every active system by one GMRES iteration or one
+ * refinement residual. */
+typedef struct eb_solver_s* eb_solver;
+int eb_solver_create(const eb_solve_options* opt, eb_solver* out);
+int eb_solver_destroy(eb_solver solver);
+int eb_solver_add(eb_solver solver, eb_mesh mesh, int nrhs, const double* b, int* ids);
+int eb_solver_step(eb_solver solver, int* nactive);
+int eb_solver_done(eb_solver solver, int id, int* done);
+int eb_solver_result(eb_solver solver, int id, double* x, eb_solve_stats* stats);
+int eb_solver_remove(eb_solver solver, int id);
+/* Device memory one system of this mesh holds in the solver (Krylov basis
+ * and vectors), for admission control. */
+int eb_solver_bytes_per_system(eb_solver solver, eb_mesh mesh, long long* bytes);
+
+/* Right-hand side of the direct (Green) formulation of the interior Dirichlet
+ * problem, as the reference examples build it (python/examples/
+ * laplace3dDirichletGPU.py:63): b = (1/2) M g + K g with M the P0 x P1 mass
+ * matrix (src/BEM3dLaplace.cpp:448-486) and K the double layer, for nrhs
+ * vertex data g ([nrhs][nnodes], host) into b ([nrhs][nelems], host). FP64. */
+int eb_dirichlet_rhs(eb_mesh mesh, int nrhs, const double* g, double* b);
+
 /* The quadrature rules behind index `order` (host only, no GPU needed):
  * the Gauss-Legendre rule on [0,1] (up to 64 points) and the triangle rule on
  * the reference triangle (up to 79 points, weights summing to 1/2). Mirrors
