@@ -21,7 +21,7 @@ import numpy as np
 
 from ._lib import EB_PREC_FP64, EB_PREC_MIXED, EasyBemError, SolveOptions, SolveStats, check, lib
 
-__all__ = ["Mesh", "Solver", "solve", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
+__all__ = ["Mesh", "Solver", "Server", "solve", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
            "apply_gpu_laplace3d_1layer_linears", "apply_gpu_laplace3d_2layer",
            "apply_gpu_laplace3d_hypersing", "version", "precision_code"]
 
@@ -213,6 +213,76 @@ class Solver:
         n = ctypes.c_longlong()
         check(lib().eb_solver_bytes_per_system(self._h, mesh.handle, ctypes.byref(n)))
         return n.value
+
+
+class Server:
+    """Continuous-batching BEM solve server (see include/easybem_gpu.h).
+
+    ``submit(nodes, elems, g)`` queues a request (g: [nrhs, nnodes] Dirichlet
+    vertex data) and returns its id; ``step()`` advances every running
+    request by one iteration; ``result(id)`` returns (t, stats, times) once
+    ``state(id) == 4``.
+    """
+
+    STATES = {0: "queued", 1: "preparing", 2: "prepared", 3: "solving", 4: "done", 5: "failed"}
+
+    def __init__(self, budget_bytes: int, max_systems: int = 4096, tol=1e-8, inner_tol=1e-6, restart=50,
+                 max_cycles=40, max_iterations=4000, inner_precision="mixed"):
+        o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision))
+        h = ctypes.c_void_p()
+        check(lib().eb_server_create(int(budget_bytes), int(max_systems), ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._shape = {}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().eb_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, nodes, elems, g, order: int = 4) -> int:
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        elems = np.ascontiguousarray(elems, dtype=np.int32)
+        g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1, nodes.shape[0])
+        rid = ctypes.c_longlong()
+        check(lib().eb_server_submit(self._h, nodes.shape[0], _ptr(nodes), elems.shape[0], _ptr(elems), int(order),
+                                     g.shape[0], _ptr(g), ctypes.byref(rid)))
+        self._shape[rid.value] = (g.shape[0], elems.shape[0])
+        return rid.value
+
+    def step(self):
+        a, w = ctypes.c_int(), ctypes.c_int()
+        check(lib().eb_server_step(self._h, ctypes.byref(a), ctypes.byref(w)))
+        return a.value, w.value
+
+    def state(self, rid: int) -> int:
+        st = ctypes.c_int()
+        check(lib().eb_server_poll(self._h, ctypes.c_longlong(rid), ctypes.byref(st)))
+        return st.value
+
+    def result(self, rid: int):
+        nrhs, ne = self._shape[rid]
+        t = np.empty((nrhs, ne))
+        stats = (SolveStats * nrhs)()
+        times = np.zeros(4)
+        check(lib().eb_server_result(self._h, ctypes.c_longlong(rid), _ptr(t), stats, _ptr(times)))
+        st = [{"converged": bool(s.converged), "cycles": s.cycles, "iterations": s.iterations,
+               "rel_residual": s.rel_residual} for s in stats]
+        return t, st, {"latency_ms": times[0], "queue_ms": times[1], "prepare_ms": times[2], "solve_ms": times[3]}
+
+    def release(self, rid: int):
+        check(lib().eb_server_release(self._h, ctypes.c_longlong(rid)))
+        self._shape.pop(rid, None)
+
+    def usage(self):
+        u, b = ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().eb_server_usage(self._h, ctypes.byref(u), ctypes.byref(b)))
+        return u.value, b.value
 
 
 def solve(problems, **options):

@@ -59,6 +59,15 @@ _SIGNATURES = {
     "eb_solver_result": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_solver_remove": (ctypes.c_int, [_dp, ctypes.c_int]),
     "eb_solver_bytes_per_system": (ctypes.c_int, [_dp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_server_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, _dp, ctypes.POINTER(_dp)]),
+    "eb_server_destroy": (ctypes.c_int, [_dp]),
+    "eb_server_submit": (ctypes.c_int, [_dp, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, _dp,
+                                        ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_server_step": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "eb_server_poll": (ctypes.c_int, [_dp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]),
+    "eb_server_result": (ctypes.c_int, [_dp, ctypes.c_longlong, _dp, _dp, _dp]),
+    "eb_server_release": (ctypes.c_int, [_dp, ctypes.c_longlong]),
+    "eb_server_usage": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "eb_last_kernel_ms": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
 }
 

@@ -219,18 +219,21 @@ static int build_near(Mesh* m)
   EB_CHECK(d_dle.alloc(sizeof(double) * 3 * std::max(npairs, 1)));
   const int nslots = (int)h.dl_col.size();
   EB_CHECK(m->dl_val.alloc(sizeof(double) * std::max(nslots, 1)));
-  if (npairs > 0) {
-    near_values_kernel<<<(npairs + 127) / 128, 128>>>(h.quad, d_nodes.as<double>(), d_elems.as<int>(),
-                                                      d_pi.as<int>(), d_pj.as<int>(), npairs,
-                                                      m->sl_val.as<double>(), d_dle.as<double>());
-    EB_CUDA(cudaGetLastError());
-  }
-  if (nslots > 0) {
-    dl_gather_kernel<<<(nslots + 255) / 256, 256>>>(d_cptr.as<int>(), d_contrib.as<int>(), d_dle.as<double>(),
-                                                   nslots, m->dl_val.as<double>());
-    EB_CUDA(cudaGetLastError());
-  }
-  EB_CUDA(cudaDeviceSynchronize());
+  // a private stream: mesh set-up overlaps work other threads run on the GPU
+  cudaStream_t st = nullptr;
+  EB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  if (npairs > 0)
+    near_values_kernel<<<(npairs + 127) / 128, 128, 0, st>>>(h.quad, d_nodes.as<double>(), d_elems.as<int>(),
+                                                             d_pi.as<int>(), d_pj.as<int>(), npairs,
+                                                             m->sl_val.as<double>(), d_dle.as<double>());
+  if (nslots > 0)
+    dl_gather_kernel<<<(nslots + 255) / 256, 256, 0, st>>>(d_cptr.as<int>(), d_contrib.as<int>(),
+                                                          d_dle.as<double>(), nslots, m->dl_val.as<double>());
+  const cudaError_t e1 = cudaGetLastError();
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  EB_CUDA(e1);
+  EB_CUDA(e2);
   return EB_OK;
 }
 

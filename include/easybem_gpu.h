@@ -140,6 +140,29 @@ int eb_solver_remove(eb_solver solver, int id);
  * and vectors), for admission control. */
 int eb_solver_bytes_per_system(eb_solver solver, eb_mesh mesh, long long* bytes);
 
+/* ---- Continuous-batching solve server (no counterpart in the reference).
+ * A request is a mesh (1-based elements, quadrature order) with nrhs sets of
+ * Dirichlet vertex data g ([nrhs][nnodes]); its answer is t ([nrhs][nelems])
+ * with V t = (1/2 M + K) g, solved to the server's options. Requests are
+ * admitted under a device-memory budget (resident mesh data plus Krylov
+ * storage), prepared by a host worker thread while other requests run, and
+ * join the shared lockstep solver as soon as they are ready and fewer than
+ * max_systems right-hand sides are active; eb_server_step advances all of
+ * them by one iteration. A request's result does not depend on what runs
+ * beside it. Poll states: 0 queued, 1 preparing, 2 prepared, 3 solving,
+ * 4 done, 5 failed. times_ms (optional, 4 entries): total latency, queue
+ * wait, preparation, solve. */
+typedef struct eb_server_s* eb_server;
+int eb_server_create(long long budget_bytes, int max_systems, const eb_solve_options* opt, eb_server* out);
+int eb_server_destroy(eb_server server);
+int eb_server_submit(eb_server server, int nnodes, const double* nodes, int nelems, const int* elems, int order,
+                     int nrhs, const double* g, long long* id);
+int eb_server_step(eb_server server, int* nactive, int* nwaiting);
+int eb_server_poll(eb_server server, long long id, int* state);
+int eb_server_result(eb_server server, long long id, double* t, eb_solve_stats* stats, double* times_ms);
+int eb_server_release(eb_server server, long long id);
+int eb_server_usage(eb_server server, long long* used_bytes, long long* budget_bytes);
+
 /* Right-hand side of the direct (Green) formulation of the interior Dirichlet
  * problem, as the reference examples build it (python/examples/
  * laplace3dDirichletGPU.py:63): b = (1/2) M g + K g with M the P0 x P1 mass

@@ -1,0 +1,110 @@
+"""Continuous-batching solve server: admission, overlap, isolation.
+
+Requests are structured tori (the serving workload) with exterior point
+sources. Checks: every request converges to the FP64 residual target; a
+request's answer is the same served alone and in a mix with late arrivals
+(<= 1e-12 relative); admission never exceeds the device-memory budget;
+oversized and invalid requests fail cleanly without disturbing the others.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from easybem_b200 import EasyBemError, meshes
+
+pytestmark = pytest.mark.gpu
+
+
+def _request(n_u, r, nrhs, seed):
+    nodes, elems = meshes.torus(n_u, r)
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(nrhs, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    src = d * rng.uniform(2.0, 3.0, size=(nrhs, 1)) * 1.5
+    g = np.stack([1.0 / np.linalg.norm(nodes - p, axis=1) for p in src])
+    return nodes, elems, g
+
+
+def _drain(srv, ids, limit=5000):
+    for _ in range(limit):
+        srv.step()
+        if all(srv.state(i) >= 4 for i in ids):
+            return
+    raise AssertionError("server did not finish")
+
+
+def test_requests_same_alone_and_in_mix(gpu_lib):
+    reqs = [_request(24, 0.3, 2, 1), _request(32, 0.25, 1, 2), _request(40, 0.35, 3, 3), _request(16, 0.2, 1, 4)]
+    # alone: a fresh server per request
+    alone = []
+    for nodes, elems, g in reqs[:2]:
+        srv = gpu_lib.Server(budget_bytes=8 << 30)
+        rid = srv.submit(nodes, elems, g)
+        _drain(srv, [rid])
+        alone.append(srv.result(rid)[0])
+        srv.close()
+    # mix: two requests first, the others arrive while those are solving
+    srv = gpu_lib.Server(budget_bytes=8 << 30)
+    ids = [srv.submit(*reqs[0]), srv.submit(*reqs[2])]
+    for _ in range(3):
+        srv.step()
+    ids += [srv.submit(*reqs[1]), srv.submit(*reqs[3])]
+    _drain(srv, ids)
+    results = {}
+    for rid in ids:
+        t, stats, times = srv.result(rid)
+        for st in stats:
+            assert st["converged"] and st["rel_residual"] <= 1e-8
+        assert times["latency_ms"] >= times["solve_ms"] > 0
+        results[rid] = t
+    assert rel_l2(results[ids[0]], alone[0]) <= 1e-12
+    assert rel_l2(results[ids[2]], alone[1]) <= 1e-12
+    srv.close()
+
+
+def test_admission_respects_memory_budget(gpu_lib):
+    reqs = [_request(64, 0.3, 2, s) for s in range(4)]
+    probe = gpu_lib.Server(budget_bytes=64 << 30)
+    rid = probe.submit(*reqs[0])
+    one, _ = probe.usage()  # the admission estimate of one request
+    _drain(probe, [rid])
+    probe.close()
+    # a budget for one request at a time (plus slack for the measured footprint)
+    budget = int(1.5 * one)
+    srv = gpu_lib.Server(budget_bytes=budget)
+    ids = [srv.submit(*r) for r in reqs]
+    peak = 0
+    for _ in range(5000):
+        srv.step()
+        used, b = srv.usage()
+        peak = max(peak, used)
+        assert used <= b
+        if all(srv.state(i) >= 4 for i in ids):
+            break
+    for rid in ids:
+        t, stats, _ = srv.result(rid)
+        assert all(st["converged"] for st in stats)
+    assert peak > 0
+    # a request larger than the whole budget is refused at submission
+    big = _request(256, 0.3, 8, 9)
+    with pytest.raises(EasyBemError) as e:
+        srv.submit(*big)
+    assert e.value.status == 4
+    srv.close()
+
+
+def test_invalid_request_fails_alone(gpu_lib):
+    good = _request(24, 0.3, 1, 5)
+    nodes, elems, g = _request(20, 0.3, 1, 6)
+    bad = elems.copy()
+    bad[0, 0] = nodes.shape[0] + 7
+    srv = gpu_lib.Server(budget_bytes=8 << 30)
+    rb = srv.submit(nodes, bad, g)
+    rg = srv.submit(*good)
+    _drain(srv, [rb, rg])
+    assert srv.state(rb) == 5
+    with pytest.raises(EasyBemError):
+        srv.result(rb)
+    t, stats, _ = srv.result(rg)
+    assert stats[0]["converged"]
+    srv.close()
