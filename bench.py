@@ -40,8 +40,8 @@ METRIC = "SL+DL Galerkin apply Gpairs/s, mixed vs FP64 at 1e-6 rel err; p99 solv
 LEVEL = 6
 SEED = 1
 ORDER = 4
-WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L6 "
-            "(81,920 triangles, 40,962 vertices), quadrature index 4 (Q=7)")
+WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L{level} "
+            "({ne:,} triangles, {nv:,} vertices), quadrature index 4 (Q=7)")
 FLOPS_PER_PAIR = 20  # SL: 3 sub + 5 (|r|^2) + 1 rsqrt + 2 fma; DL: 5 (r.p) + 2 mul + 2 fma (FMA = 2)
 
 
@@ -53,6 +53,14 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--level", type=int, default=LEVEL)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="matvec", choices=["matvec", "batch", "serve", "large", "small"],
+                   help="matvec: the headline single-mesh SL+DL apply (default); batch: 256 uneven "
+                        "ellipsoids x 4 RHS, batched apply and GMRES-IR solves; serve: Poisson stream of "
+                        "torus solves, p50/p99 latency; large: icosphere L7 apply and solve; small: "
+                        "icosphere L3 Dirichlet solve")
+    p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
+    p.add_argument("--serve-sample", type=int, default=32,
+                   help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
     return p.parse_args()
 
 
@@ -179,7 +187,8 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": "Gpairs/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "sample_rows_per_step": len(rows)},
+            "data": "synthetic", "config": {"workload": WORKLOAD.format(level=args.level, ne=ne, nv=nodes.shape[0]),
+                                            "sample_rows_per_step": len(rows)},
             "cpu_baseline": {"value": value, "unit": "Gpairs/s", "cores": ncores, "kind": kind,
                              "sample": f"{len(rows)} of {ne} rows per step, reference FP64 pair routines "
                                        f"(src/BEM3dLaplace.cpp:22-437) with OpenMP"},
@@ -187,10 +196,165 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def serve_stream(n, seed=0):
+    from easybem_b200 import meshes
+    return list(meshes.serving_stream(n, rate=200.0, seed=seed))
+
+
+def run_serve(args):
+    """Serving: 2,000 torus solve requests, Poisson arrivals at 200/s, 120 GB budget."""
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    from easybem_b200.serving import run_stream
+    reqs = serve_stream(args.requests, seed=rank)
+    res = run_stream(reqs, budget_bytes=120 * 10 ** 9, tol=1e-8)
+    res.pop("results", None)
+    if rank == 0:
+        line = {"metric": METRIC, "workload": "serve", "value": res["p99_ms"], "unit": "ms (p99 request latency)",
+                "higher_is_better": False, "n_gpus": world, "data": "synthetic",
+                "config": {"workload": "2,000 torus Dirichlet solves (512-32,768 triangles, 1-8 RHS), Poisson "
+                                       "arrivals at 200/s, 120 GB admission budget, tol 1e-8",
+                           "requests": args.requests},
+                **{k: v for k, v in res.items()}}
+        print(json.dumps(line), flush=True)
+
+
+def run_batch(args):
+    """256 closed surfaces (icosphere L2-L5 ellipsoids) x 4 RHS: batched applies and solves."""
+    import torch
+    import easybem_b200 as eb
+    from easybem_b200 import meshes
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    items = meshes.ellipsoid_batch(256, seed=3, levels=(2, 3, 4, 5), nrhs=4)
+    t0 = time.perf_counter()
+    ms = [eb.Mesh(it["nodes"], it["elems"]) for it in items]
+    t_create = time.perf_counter() - t0
+    rhs = [m.dirichlet_rhs(np.stack([1.0 / np.linalg.norm(it["nodes"] - p, axis=1) for p in it["sources"]]))
+           for m, it in zip(ms, items)]
+    dev = torch.device("cuda", local)
+    d_t = [torch.from_numpy(np.ascontiguousarray(b)).to(dev) for b in rhs]
+    d_v = [torch.empty_like(x) for x in d_t]
+    out = {}
+    for prec in ("mixed", "fp64"):
+        bt = eb.Batch(ms, 4, prec)
+        st = torch.cuda.current_stream()
+        for _ in range(2):
+            bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v], st.cuda_stream)
+        k = 3 if prec == "mixed" else 2
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(k):
+            bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v], st.cuda_stream)
+        b.record(st)
+        torch.cuda.synchronize()
+        ms_apply = a.elapsed_time(b) / k
+        out[prec] = {"ms_per_apply": ms_apply, "Gpairs_per_s": bt.quad_pairs / (ms_apply * 1e-3) / 1e9,
+                     "rhs_evals_per_s_G": 4 * bt.quad_pairs / (ms_apply * 1e-3) / 1e9}
+        bt.close()
+    t0 = time.perf_counter()
+    res = eb.solve(list(zip(ms, rhs)), tol=1e-8)
+    t_solve = time.perf_counter() - t0
+    stats = [s for _, sl in res for s in sl]
+    line = {"metric": METRIC, "workload": "batch", "value": out["mixed"]["Gpairs_per_s"], "unit": "Gpairs/s",
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "256 ellipsoids (icosphere L2-L5, 320-20,480 triangles), 4 RHS each, "
+                                   "batched SL apply + GMRES(50)-IR to 1e-8",
+                       "quad_pairs_per_apply": int(sum(m.far_quad_pairs for m in ms))},
+            "apply_mixed": out["mixed"], "apply_fp64": out["fp64"],
+            "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
+            "mesh_setup_s": t_create, "solve_s": t_solve, "systems": len(stats),
+            "solves_per_s": len(stats) / t_solve, "converged": sum(s["converged"] for s in stats),
+            "max_rel_residual": max(s["rel_residual"] for s in stats),
+            "iterations_mean": float(np.mean([s["iterations"] for s in stats])),
+            "cycles_mean": float(np.mean([s["cycles"] for s in stats]))}
+    print(json.dumps(line), flush=True)
+
+
+def run_large(args):
+    """Icosphere L7 (327,680 triangles): SL+DL apply in both precisions and a GMRES-IR solve."""
+    import torch
+    import easybem_b200 as eb
+    from oracle.oracle import Oracle
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    nodes, elems, t, u = make_problem(7)
+    t0 = time.perf_counter()
+    m = eb.Mesh(nodes, elems)
+    t_create = time.perf_counter() - t0
+    m.set_profiling(True)
+    res = {}
+    for prec in ("mixed", "fp64"):
+        m.apply_sl_dl(t, u, precision=prec)
+        v, q = m.apply_sl_dl(t, u, precision=prec)
+        far, fin = m.last_kernel_ms()
+        res[prec] = (v, q, far, fin)
+    rng = np.random.default_rng(5)
+    rows = np.sort(rng.choice(elems.shape[0], 16, replace=False)).astype(np.int32)
+    vo, qo = Oracle(ORDER).apply_rows(nodes, elems, t, u, rows)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
+    b = m.dirichlet_rhs(g)
+    t0 = time.perf_counter()
+    [(x, st)] = eb.solve([(m, b)], tol=1e-8)
+    t_solve = time.perf_counter() - t0
+    pairs = m.far_quad_pairs
+    line = {"metric": METRIC, "workload": "large", "value": pairs / (res["mixed"][2] * 1e-3) / 1e9,
+            "unit": "Gpairs/s", "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "radius-perturbed icosphere L7 (327,680 triangles, 163,842 vertices)",
+                       "quad_pairs_per_step": pairs, "near_pairs": m.near_pairs},
+            "mesh_setup_s": t_create,
+            "mixed": {"far_ms": res["mixed"][2], "finalize_ms": res["mixed"][3]},
+            "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
+                     "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
+            "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed"][0][rows], vo), "mixed_dl": rel(res["mixed"][1][rows], qo),
+                                  "fp64_sl": rel(res["fp64"][0][rows], vo), "fp64_dl": rel(res["fp64"][1][rows], qo),
+                                  "oracle_rows": len(rows)},
+            "solve": {"seconds": t_solve, **st[0]}}
+    print(json.dumps(line), flush=True)
+
+
+def run_small(args):
+    """Icosphere L3 (1,280 triangles): Dirichlet solve, g = 1/|x - (0,0,3)|, checked against the reference."""
+    import torch
+    import easybem_b200 as eb
+    from easybem_b200 import meshes
+    from oracle import oracle as O
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    nodes, elems = meshes.icosphere(3)
+    g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
+    t0 = time.perf_counter()
+    m = eb.Mesh(nodes, elems)
+    b = m.dirichlet_rhs(g)
+    [(x, st)] = eb.solve([(m, b)], tol=1e-8)
+    t_gpu = time.perf_counter() - t0
+    rel = lambda a, c: float(np.linalg.norm(a - c) / np.linalg.norm(c))
+    line = {"metric": METRIC, "workload": "small", "value": 1e3 * t_gpu, "unit": "ms (mesh + RHS + solve)",
+            "higher_is_better": False, "data": "synthetic",
+            "config": {"workload": "unit icosphere L3 (1,280 triangles), Dirichlet g = 1/|x-(0,0,3)|"},
+            "solve": st[0]}
+    rng = np.random.default_rng(0)
+    dens = rng.normal(size=elems.shape[0])
+    if O.ref_available():
+        t0 = time.perf_counter()
+        V, K, D, M = O.ref_dense(nodes, elems, ORDER)
+        x_ref = np.linalg.solve(V, (0.5 * M + K) @ g)
+        line["reference_cpu_dense_s"] = time.perf_counter() - t0
+        line["rel_err_solution_vs_reference"] = rel(x, x_ref)
+        line["rel_err_matvec_vs_reference"] = rel(m.apply_sl(dens), V @ dens)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "matvec":
+        {"batch": run_batch, "serve": run_serve, "large": run_large, "small": run_small}[args.workload](args)
         return
     rank, world, local = dist_env()
     import torch
@@ -315,11 +479,16 @@ def main():
     near_bytes = 12 * mesh.near_pairs + 8 * ne * 13 * 3  # SL CSR + DL CSR values/cols (approx.)
     cpu = None if args.no_cpu_baseline else cpu_reference_sample(nodes, elems, t, u)
     clocks = sampler.summary()
+    serve = None
+    if args.serve_sample > 0 and world == 1:
+        from easybem_b200.serving import run_stream
+        serve = run_stream(serve_stream(args.serve_sample), budget_bytes=120 * 10 ** 9, tol=1e-8)
+        serve.pop("results", None)
     line = {
         "metric": METRIC, "value": value, "unit": "Gpairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 far field / f64 near field", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "triangles": ne, "vertices": nv, "quad_pairs_per_step": pairs,
+        "config": {"workload": WORKLOAD.format(level=args.level, ne=ne, nv=nv), "triangles": ne, "vertices": nv, "quad_pairs_per_step": pairs,
                    "near_pairs": mesh.near_pairs, "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MB write)"},
         "fp64": {"value": value64, "unit": "Gpairs/s", "ms_per_step": step_ms64, "steps": len(ms_fp64),
@@ -340,6 +509,12 @@ def main():
     }
     if cpu is not None:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if serve is not None:
+        line["serve_sample"] = {"requests": serve["requests"], "p50_ms": serve["p50_ms"], "p99_ms": serve["p99_ms"],
+                                "solves_per_s": serve["solves_per_s"], "converged": serve["converged"],
+                                "max_rel_residual": serve["max_rel_residual"],
+                                "note": "first requests of the 2,000-request Poisson stream (200/s); "
+                                        "full stream: bench.py --workload serve"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

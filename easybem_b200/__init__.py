@@ -21,7 +21,7 @@ import numpy as np
 
 from ._lib import EB_PREC_FP64, EB_PREC_MIXED, EasyBemError, SolveOptions, SolveStats, check, lib
 
-__all__ = ["Mesh", "Solver", "Server", "solve", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
+__all__ = ["Mesh", "Batch", "Solver", "Server", "solve", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
            "apply_gpu_laplace3d_1layer_linears", "apply_gpu_laplace3d_2layer",
            "apply_gpu_laplace3d_hypersing", "version", "precision_code"]
 
@@ -152,6 +152,41 @@ class Mesh:
         a, b = ctypes.c_double(), ctypes.c_double()
         check(lib().eb_last_kernel_ms(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+
+class Batch:
+    """P0 single-layer applies of many meshes x ncols right-hand sides in one launch.
+
+    ``apply_device(d_t, d_v, stream)`` takes lists of device pointers (one
+    [ncols][nelems] array per mesh).
+    """
+
+    def __init__(self, meshes, ncols: int = 1, precision="mixed"):
+        arr = (ctypes.c_void_p * len(meshes))(*[m.handle.value for m in meshes])
+        h = ctypes.c_void_p()
+        check(lib().eb_batch_create(len(meshes), arr, int(ncols), precision_code(precision), ctypes.byref(h)))
+        self._h = h
+        self.meshes = list(meshes)
+        self.ncols = ncols
+        q = ctypes.c_longlong()
+        check(lib().eb_batch_info(h, ctypes.byref(q)))
+        self.quad_pairs = q.value
+
+    def apply_device(self, d_t, d_v, stream=0):
+        n = len(self.meshes)
+        check(lib().eb_batch_apply(self._h, (ctypes.c_void_p * n)(*d_t), (ctypes.c_void_p * n)(*d_v),
+                                   ctypes.c_void_p(stream or None)))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().eb_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Solver:

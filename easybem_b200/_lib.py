@@ -59,6 +59,10 @@ _SIGNATURES = {
     "eb_solver_result": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_solver_remove": (ctypes.c_int, [_dp, ctypes.c_int]),
     "eb_solver_bytes_per_system": (ctypes.c_int, [_dp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_batch_create": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp)]),
+    "eb_batch_destroy": (ctypes.c_int, [_dp]),
+    "eb_batch_apply": (ctypes.c_int, [_dp, _dp, _dp, _dp]),
+    "eb_batch_info": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong)]),
     "eb_server_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, _dp, ctypes.POINTER(_dp)]),
     "eb_server_destroy": (ctypes.c_int, [_dp]),
     "eb_server_submit": (ctypes.c_int, [_dp, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, _dp,

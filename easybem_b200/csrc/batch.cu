@@ -134,3 +134,82 @@ int Batch::run_graph(cudaStream_t st)
 }
 
 }  // namespace eb
+
+// ---------------------------------------------------------------------------
+// C ABI: batched applies over a fixed set of meshes.
+
+eb::Mesh* eb_mesh_internal(eb_mesh handle);
+
+struct eb_batch_s {
+  std::vector<std::unique_ptr<eb::BatchEntry>> entries;
+  eb::Batch batch;
+  eb::DevBuf flags;
+  cudaStream_t stream = nullptr;
+  int ncols = 1;
+};
+
+using eb::set_error;
+
+extern "C" {
+
+int eb_batch_create(int nmesh, const eb_mesh* meshes, int ncols, int precision, eb_batch* out)
+{
+  if (!out || nmesh < 1 || !meshes || ncols < 1 || ncols > eb::kBatchCols)
+    return set_error(EB_ERR_INVALID, "need >= 1 mesh and 1..4 columns");
+  if (precision != EB_PREC_FP64 && precision != EB_PREC_MIXED)
+    return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
+  auto b = std::make_unique<eb_batch_s>();
+  b->ncols = ncols;
+  std::vector<eb::BatchEntry*> ents;
+  for (int i = 0; i < nmesh; i++) {
+    if (!meshes[i]) return set_error(EB_ERR_INVALID, "null mesh");
+    auto e = std::make_unique<eb::BatchEntry>();
+    EB_CHECK(eb::batch_entry_init(e.get(), eb_mesh_internal(meshes[i])));
+    ents.push_back(e.get());
+    b->entries.push_back(std::move(e));
+  }
+  EB_CHECK(b->flags.alloc(sizeof(int) * nmesh));
+  std::vector<int> ones(nmesh, 1);
+  EB_CUDA(cudaMemcpy(b->flags.p, ones.data(), sizeof(int) * nmesh, cudaMemcpyHostToDevice));
+  EB_CHECK(b->batch.build(ents, precision == EB_PREC_MIXED, ncols, b->flags.as<int>()));
+  EB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  *out = b.release();
+  return EB_OK;
+}
+
+int eb_batch_destroy(eb_batch b)
+{
+  if (!b) return EB_OK;
+  if (b->stream) {
+    cudaStreamSynchronize(b->stream);
+    cudaStreamDestroy(b->stream);
+  }
+  delete b;
+  return EB_OK;
+}
+
+int eb_batch_apply(eb_batch b, const double* const* d_t, double* const* d_v, void* stream)
+{
+  if (!b || !d_t || !d_v) return set_error(EB_ERR_INVALID, "null argument");
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  for (size_t i = 0; i < b->entries.size(); i++) {
+    const size_t bytes = sizeof(double) * (size_t)b->ncols * b->entries[i]->mesh->h.ne;
+    EB_CUDA(cudaMemcpyAsync(b->entries[i]->tin.p, d_t[i], bytes, cudaMemcpyDeviceToDevice, st));
+  }
+  EB_CHECK(b->batch.run_graph(st));
+  for (size_t i = 0; i < b->entries.size(); i++) {
+    const size_t bytes = sizeof(double) * (size_t)b->ncols * b->entries[i]->mesh->h.ne;
+    EB_CUDA(cudaMemcpyAsync(d_v[i], b->entries[i]->vout.p, bytes, cudaMemcpyDeviceToDevice, st));
+  }
+  if (!stream) EB_CUDA(cudaStreamSynchronize(st));
+  return EB_OK;
+}
+
+int eb_batch_info(eb_batch b, long long* quad_pairs)
+{
+  if (!b) return set_error(EB_ERR_INVALID, "null batch");
+  if (quad_pairs) *quad_pairs = b->batch.quad_pairs();
+  return EB_OK;
+}
+
+}  // extern "C"

@@ -141,14 +141,41 @@ def torus(n_u: int, r_minor: float, r_major: float = 1.0):
     y = (r_major + r_minor * np.cos(W)) * np.sin(U)
     z = r_minor * np.sin(W)
     nodes = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
-    idx = lambda i, j: (i % n_u) * n_v + (j % n_v)
-    tris = []
-    for i in range(n_u):
-        for j in range(n_v):
-            a, b, c, d = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
-            tris.append((a, b, c))
-            tris.append((a, c, d))
-    return nodes, (np.array(tris, dtype=np.int64) + 1).astype(np.int32)
+    i, j = np.meshgrid(np.arange(n_u), np.arange(n_v), indexing="ij")
+    i, j = i.ravel(), j.ravel()
+    a = i * n_v + j
+    b = ((i + 1) % n_u) * n_v + j
+    c = ((i + 1) % n_u) * n_v + (j + 1) % n_v
+    d = i * n_v + (j + 1) % n_v
+    tris = np.empty((2 * len(a), 3), dtype=np.int64)
+    tris[0::2] = np.stack([a, b, c], 1)
+    tris[1::2] = np.stack([a, c, d], 1)
+    return nodes, (tris + 1).astype(np.int32)
+
+
+def serving_stream(n: int = 2000, rate: float = 200.0, seed: int = 0, nu_range=(32, 256),
+                   r_range=(0.2, 0.4), nrhs_range=(1, 8)):
+    """The serving workload: Poisson arrivals of torus Dirichlet solves.
+
+    Request k arrives at the k-th event of a Poisson process of rate ``rate``
+    per second; its torus has major radius 1, minor radius ~U[r_range],
+    n_u ~ U{nu_range} (n_v = n_u/4) and 1..8 right-hand sides from exterior
+    point sources at distance ~U[2, 4] x (1 + r) from the origin. Yields dicts
+    with ``t_arrival``, ``nodes``, ``elems`` (1-based) and ``g`` [nrhs, nnodes].
+    """
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    for _ in range(n):
+        t += rng.exponential(1.0 / rate)
+        n_u = int(rng.integers(nu_range[0], nu_range[1] + 1))
+        r = float(rng.uniform(*r_range))
+        nrhs = int(rng.integers(nrhs_range[0], nrhs_range[1] + 1))
+        nodes, elems = torus(n_u, r)
+        d = rng.normal(size=(nrhs, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        src = d * rng.uniform(2.0, 4.0, size=(nrhs, 1)) * (1.0 + r)
+        g = np.stack([1.0 / np.linalg.norm(nodes - p, axis=1) for p in src])
+        yield dict(t_arrival=t, nodes=nodes, elems=elems, g=g, n_u=n_u, r_minor=r)
 
 
 def point_source_data(nodes, elems, src):

@@ -92,6 +92,19 @@ int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double*
 int eb_apply_hypersingular_device(eb_mesh mesh, int precision, const double* d_u, double* d_q,
                                   void* stream);
 
+/* ---- Batched apply (no counterpart in the reference): the P0 single layer
+ * of many meshes, each with ncols (1..4) right-hand sides, in one persistent
+ * far-field launch (captured once in a CUDA graph and replayed). d_t[i] and
+ * d_v[i] are device arrays [ncols][nelems_i]. With a null stream the call
+ * runs on the batch's own stream and returns when done; otherwise it is
+ * asynchronous on `stream`. */
+typedef struct eb_batch_s* eb_batch;
+int eb_batch_create(int nmesh, const eb_mesh* meshes, int ncols, int precision, eb_batch* out);
+int eb_batch_destroy(eb_batch batch);
+int eb_batch_apply(eb_batch batch, const double* const* d_t, double* const* d_v, void* stream);
+/* Regular quadrature-point pairs one batched apply evaluates (per column set). */
+int eb_batch_info(eb_batch batch, long long* quad_pairs);
+
 /* ---- Solves: V x = b (P0 single layer) by GMRES with iterative refinement.
  * No counterpart in the reference (its drivers call SciPy CG on FP32 GPU
  * matvecs, python/examples/laplace3dDirichletGPU.py:64-81). Each restart

@@ -162,3 +162,27 @@ def test_hypersingular_properties_large(gpu_lib):
         assert abs(u2 @ d1 - u1 @ d2) < 1e-6 * abs(u1 @ d1)
         # D is positive semi-definite
         assert u1 @ d1 > 0
+
+
+def test_batched_apply_equals_per_mesh_applies(gpu_lib):
+    import torch
+    batch = meshes.ellipsoid_batch(6, seed=21, levels=(1, 2, 3), nrhs=4)
+    ms = [gpu_lib.Mesh(b["nodes"], b["elems"]) for b in batch]
+    rng = np.random.default_rng(8)
+    for ncols in (1, 3, 4):
+        for prec in ("mixed", "fp64"):
+            ts = [rng.normal(size=(ncols, m.nelems)) for m in ms]
+            d_t = [torch.from_numpy(t).cuda() for t in ts]
+            d_v = [torch.empty_like(x) for x in d_t]
+            bt = gpu_lib.Batch(ms, ncols, prec)
+            for _ in range(2):  # the second call replays the captured graph
+                bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v])
+                torch.cuda.synchronize()
+                for m, t, v in zip(ms, ts, d_v):
+                    vv = v.cpu().numpy()
+                    for c in range(ncols):
+                        ref = m.apply_sl(t[c], precision=prec)
+                        assert rel_l2(vv[c], ref) <= (1e-14 if prec == "fp64" else 1e-7)
+            bt.close()
+    for m in ms:
+        m.close()
