@@ -43,6 +43,9 @@ ORDER = 4
 WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L{level} "
             "({ne:,} triangles, {nv:,} vertices), quadrature index 4 (Q=7)")
 FLOPS_PER_PAIR = 20  # SL: 3 sub + 5 (|r|^2) + 1 rsqrt + 2 fma; DL: 5 (r.p) + 2 mul + 2 fma (FMA = 2)
+# DRAM bytes (read + write) of one far-field launch on the L6 workload, from the ncu capture
+# summarised in profiles/far_kernel_f32_sl_dl_icosphere_L6.md (39.64 MB read + 0.76 MB written).
+FAR_TRAFFIC_L6 = 39.64e6 + 0.76e6
 
 
 def parse():
@@ -499,7 +502,8 @@ def main():
                 "d2h_bytes_per_step": 16 * ne, "ms_per_step": 1e3 * e2e_s},
         "gpu_launches": 3 * args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                     "frac": achieved / peak_tflops if peak_tflops else None, "traffic": None,
+                     "frac": achieved / peak_tflops if peak_tflops else None,
+                     "traffic": FAR_TRAFFIC_L6 if args.level == LEVEL else None, "traffic_unit": "bytes per launch",
                      "kernel": "far_kernel<float,7,7,1,true>", "far_ms": far_avg,
                      "flops_per_pair": FLOPS_PER_PAIR,
                      "peak_source": "FP32 FFMA-chain calibration kernel measured in this run"},
