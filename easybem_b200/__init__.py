@@ -136,6 +136,16 @@ class Mesh:
                                           ctypes.c_void_p(d_u or None), ctypes.c_void_p(d_v or None),
                                           ctypes.c_void_p(d_q or None), ctypes.c_void_p(stream or None)))
 
+    def evaluate(self, points, t, u, precision="fp64"):
+        """u(x) = V t - W u at points [n, 3] off the surface (representation formula)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        t = _vec(t, self.nelems, "t")
+        u = _vec(u, self.nnodes, "u")
+        out = np.empty(pts.shape[0])
+        check(lib().eb_evaluate_potential(self._h, precision_code(precision), pts.shape[0], _ptr(pts), _ptr(t),
+                                          _ptr(u), _ptr(out)))
+        return out
+
     def dirichlet_rhs(self, g):
         """b = (1/2) M g + K g for vertex data g ([nnodes] or [nrhs, nnodes]), FP64."""
         g = np.ascontiguousarray(g, dtype=np.float64)

@@ -42,6 +42,7 @@ _SIGNATURES = {
     "eb_apply_sl_dl_device": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]),
     "eb_apply_sl_dl_noalloc": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp]),
     "eb_apply_sl_p1": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_apply_sl_p1_device": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp]),
     "eb_apply_hypersingular": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_apply_hypersingular_device": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp]),
     "eb_quadrature": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp,
@@ -49,6 +50,7 @@ _SIGNATURES = {
     "eb_measure_fp32_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "eb_set_profiling": (ctypes.c_int, [_dp, ctypes.c_int]),
     "eb_dirichlet_rhs": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_evaluate_potential": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]),
     "eb_solve_options_default": (None, [_dp]),
     "eb_solve_sl": (ctypes.c_int, [ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]),
     "eb_solver_create": (ctypes.c_int, [_dp, ctypes.POINTER(_dp)]),

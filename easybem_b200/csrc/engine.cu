@@ -99,7 +99,8 @@ static int build_static(Mesh* m)
   HostMesh& h = m->h;
   const int ne = h.ne, Q = h.Q, K = h.K;
   const int ntt = (h.nitems + kTT - 1) / kTT;
-  std::vector<float4> pos32((size_t)ne * Q), tgt32((size_t)h.nitems * K);
+  std::vector<float4> pos32((size_t)ne * Q), tgt32((size_t)h.nitems * K), tgtw32((size_t)h.nitems * K);
+  std::vector<dq> tgtw64((size_t)h.nitems * K);
   std::vector<dq> pos64((size_t)ne * Q), trin(ne), tgt64((size_t)h.nitems * K), tcent(h.nitems), tnrm(h.nitems),
       ccent(h.ncells), snrm(ne), ttile(ntt), splane64(ne);
   std::vector<float4> splane32(ne);
@@ -161,6 +162,10 @@ static int build_static(Mesh* m)
         const d3 xr = x - cen;
         tgt64[(size_t)item * K + a] = dq{xr.x, xr.y, xr.z, wa};
         tgt32[(size_t)item * K + a] = make_float4((float)xr.x, (float)xr.y, (float)xr.z, (float)wa);
+        // P1 test weights w_a (1 - xi - eta, xi, eta) in the triangle's vertex order
+        const double ph0 = 1.0 - h.quad.tx[pp] - h.quad.ty[pp], ph1 = h.quad.tx[pp], ph2 = h.quad.ty[pp];
+        tgtw64[(size_t)item * K + a] = dq{wa * ph0, wa * ph1, wa * ph2, 0.0};
+        tgtw32[(size_t)item * K + a] = make_float4((float)(wa * ph0), (float)(wa * ph1), (float)(wa * ph2), 0.0f);
       }
     }
   }
@@ -188,6 +193,8 @@ static int build_static(Mesh* m)
   EB_CHECK(upload(m->bary, bary));
   EB_CHECK(upload(m->tgt32, tgt32));
   EB_CHECK(upload(m->tgt64, tgt64));
+  EB_CHECK(upload(m->tgtw32, tgtw32));
+  EB_CHECK(upload(m->tgtw64, tgtw64));
   EB_CHECK(upload(m->tcent, tcent));
   EB_CHECK(upload(m->tnrm, tnrm));
   EB_CHECK(upload(m->snrm, snrm));
@@ -333,6 +340,8 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec,
   FarMeshDesc desc;
   desc.tgt32 = m->tgt32.as<float4>();
   desc.tgt64 = m->tgt64.as<dq>();
+  desc.tgtw32 = m->tgtw32.as<float4>();
+  desc.tgtw64 = m->tgtw64.as<dq>();
   desc.tcent = m->tcent.as<dq>();
   desc.tnrm = m->tnrm.as<dq>();
   desc.snrm = m->snrm.as<dq>();
@@ -566,6 +575,31 @@ int eb_quadrature(int order, int* nline, double* lx, double* lw, int* ntri, doub
   return EB_OK;
 }
 
+int eb_evaluate_potential(eb_mesh mesh, int precision, int npts, const double* pts, const double* t, const double* u,
+                          double* out)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  if (npts < 0 || (npts > 0 && (!pts || !t || !u || !out))) return set_error(EB_ERR_INVALID, "null argument");
+  if (npts == 0) return EB_OK;
+  std::lock_guard<std::mutex> g(mesh->lock);
+  eb::Mesh* m = mesh->m;
+  EB_CUDA(cudaSetDevice(m->device));
+  cudaStream_t st = mesh->stream;
+  const int ne = m->h.ne, nv = m->h.nv;
+  EB_CHECK(m->io_t.alloc(sizeof(double) * ne));
+  EB_CHECK(m->io_u.alloc(sizeof(double) * nv));
+  EB_CHECK(m->io_pts.alloc(sizeof(double) * 3 * (size_t)npts));
+  EB_CHECK(m->io_pot.alloc(sizeof(double) * (size_t)npts));
+  EB_CUDA(cudaMemcpyAsync(m->io_t.p, t, sizeof(double) * ne, cudaMemcpyHostToDevice, st));
+  EB_CUDA(cudaMemcpyAsync(m->io_u.p, u, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+  EB_CUDA(cudaMemcpyAsync(m->io_pts.p, pts, sizeof(double) * 3 * (size_t)npts, cudaMemcpyHostToDevice, st));
+  EB_CHECK(eb::mesh_evaluate_potential(m, precision, npts, m->io_pts.as<double>(), m->io_t.as<double>(),
+                                       m->io_u.as<double>(), m->io_pot.as<double>(), st));
+  EB_CUDA(cudaMemcpyAsync(out, m->io_pot.p, sizeof(double) * (size_t)npts, cudaMemcpyDeviceToHost, st));
+  EB_CUDA(cudaStreamSynchronize(st));
+  return EB_OK;
+}
+
 int eb_set_profiling(eb_mesh mesh, int on)
 {
   if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
@@ -587,10 +621,29 @@ int eb_last_kernel_ms(eb_mesh mesh, double* far_ms, double* finalize_ms)
   return EB_OK;
 }
 
+int eb_apply_sl_p1_device(eb_mesh mesh, int precision, const double* d_t, double* d_v, void* stream)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  EB_CUDA(cudaSetDevice(mesh->m->device));
+  return eb::mesh_apply_sl_p1(mesh->m, precision, d_t, d_v, (cudaStream_t)stream);
+}
+
 int eb_apply_sl_p1(eb_mesh mesh, int precision, const double* t, double* v)
 {
-  (void)mesh; (void)precision; (void)t; (void)v;
-  return set_error(EB_ERR_STATE, "eb_apply_sl_p1 is not available in this build yet");
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  if (!t || !v) return set_error(EB_ERR_INVALID, "null vector");
+  std::lock_guard<std::mutex> g(mesh->lock);
+  eb::Mesh* m = mesh->m;
+  EB_CUDA(cudaSetDevice(m->device));
+  const int nv = m->h.nv, ne = m->h.ne;
+  cudaStream_t st = mesh->stream;
+  EB_CHECK(m->io_u.alloc(sizeof(double) * nv));
+  EB_CHECK(m->io_q.alloc(sizeof(double) * std::max(nv, ne)));
+  EB_CUDA(cudaMemcpyAsync(m->io_u.p, t, sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+  EB_CHECK(eb::mesh_apply_sl_p1(m, precision, m->io_u.as<double>(), m->io_q.as<double>(), st));
+  EB_CUDA(cudaMemcpyAsync(v, m->io_q.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+  EB_CUDA(cudaStreamSynchronize(st));
+  return EB_OK;
 }
 
 int eb_apply_hypersingular_device(eb_mesh mesh, int precision, const double* d_u, double* d_q, void* stream)

@@ -10,9 +10,10 @@
 
 namespace eb {
 
+// p1t selects P1 test functions (three outputs per item; NSL = 1, no DL).
 cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
-                       int* dc, size_t smem, int grid, cudaStream_t st);
-int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem);
+                       int* dc, size_t smem, int grid, cudaStream_t st, bool p1t = false);
+int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem, bool p1t = false);
 bool far_variant_supported(int NSL, bool DL);
 cudaError_t prep_launch(bool fp32, int NSL, bool DL, const ApplyArgs& A, cudaStream_t st);
 cudaError_t finalize_launch(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st);
@@ -51,7 +52,9 @@ struct Mesh {
 
   // static geometry (sorted order)
   DevBuf pos32, pos64, wj, trin, svid, perm, iperm, bary;
-  DevBuf tgt32, tgt64, tcent, tnrm, tvid, ccent, snrm, ttile, splane32, splane64;
+  DevBuf tgt32, tgt64, tgtw32, tgtw64, tcent, tnrm, tvid, ccent, snrm, ttile, splane32, splane64;
+  // P1 x P1 single layer near field (built on first use)
+  DevBuf p1_rowptr, p1_col, p1_val;
   // near field
   DevBuf sl_rowptr, sl_col, sl_val, dl_rowptr, dl_col, dl_val;
   long long npairs = 0;
@@ -61,6 +64,8 @@ struct Mesh {
   DevBuf io_t, io_u, io_v, io_q;
   // hypersingular: curl coefficients, vertex -> (triangle, local) lists, work vectors
   DevBuf curl9, vtri_ptr, vtri_list, elems0, hs_x, hs_w;
+  // potential evaluation: per-chunk partial sums and host-call staging
+  DevBuf pot_partial, io_pts, io_pot;
   int nitems_work = 0;
   FarPlan plan;
   // one immutable device descriptor and launch shape per far-field variant
@@ -92,6 +97,13 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec,
 int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
                double* d_q, cudaStream_t st);
 
+// u(x) = V t - W u at npts points (device arrays: pts [npts][3], t [nelems], u [nnodes]).
+int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pts, const double* d_t,
+                            const double* d_u, double* d_out, cudaStream_t st);
+// v = V1 t, P1 x P1 single layer; t and v have nnodes entries (device).
+int mesh_apply_sl_p1(Mesh* m, int precision, const double* d_t, double* d_v, cudaStream_t st);
+// vertex -> (triangle, local index) lists on the device (built on first use)
+int ensure_vertex_lists(Mesh* m);
 // q = D u (hypersingular, curl form); u and q have nnodes entries (device).
 int mesh_apply_hypersingular(Mesh* m, int precision, const double* d_u, double* d_q, cudaStream_t st);
 

@@ -158,7 +158,9 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
   }
 }
 
-template <typename T, int K, int NQ, int NSL, bool DL>
+// P1T: P1 test functions; the item's three outputs are sum_a w_a phi_k(x_a) acc_a
+// (k = 0, 1, 2 in the triangle's vertex order) of the single SL charge.
+template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
 __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MINB : EB_F64_MINB)
     far_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
                int* __restrict__ counter)
@@ -167,6 +169,8 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
   constexpr bool F32 = std::is_same<T, float>::value;
   constexpr int NREC = rec_slots(NSL, DL);
   constexpr int NS = NSL > 0 ? NSL : 1;
+  constexpr int NACC = P1T ? 3 : NS + 1;
+  static_assert(!P1T || (NSL == 1 && !DL), "P1 test functions pair with one SL charge");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ int4 s_vid[kTS];
@@ -213,9 +217,9 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
     const int4 tv = active ? md.tvid[tsel] : make_int4(-1, -1, -1, 0);
 
     // float-float accumulators (FP32) or plain doubles (FP64) per output
-    T acc_hi[NS + 1], acc_lo[NS + 1];
+    T acc_hi[NACC], acc_lo[NACC];
 #pragma unroll
-    for (int c = 0; c <= NS; ++c) { acc_hi[c] = 0; acc_lo[c] = 0; }
+    for (int c = 0; c < NACC; ++c) { acc_hi[c] = 0; acc_lo[c] = 0; }
 
     const int sb = w.cell0 * kCell;
     const int se = min(md.ne, w.cell1 * kCell);
@@ -267,19 +271,35 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
           else
             eval_cell<T, K, NQ, NSL, DL, false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
                                                 cen, nrm, sl, dl);
+          if constexpr (P1T) {
 #pragma unroll
-          for (int c = 0; c <= NS; ++c) {
-            if (c == NS && !DL) break;
-            if (c < NS && NSL == 0) continue;
-            T part = 0;
+            for (int k = 0; k < 3; ++k) {
+              T part = 0;
 #pragma unroll
-            for (int a = 0; a < K; ++a) {
-              T px, py, pz, pw;
-              target(a, px, py, pz, pw);
-              part += pw * (c < NS ? sl[c][a] : dl[a]);
+              for (int a = 0; a < K; ++a) {
+                T wk;
+                if constexpr (F32) wk = comp(md.tgtw32[(size_t)tsel * K + a], k);
+                else wk = comp(md.tgtw64[(size_t)tsel * K + a], k);
+                part += wk * sl[0][a];
+              }
+              if constexpr (F32) two_sum_add(acc_hi[k], acc_lo[k], part);
+              else acc_hi[k] += part;
             }
-            if constexpr (F32) two_sum_add(acc_hi[c], acc_lo[c], part);
-            else acc_hi[c] += part;
+          } else {
+#pragma unroll
+            for (int c = 0; c <= NS; ++c) {
+              if (c == NS && !DL) break;
+              if (c < NS && NSL == 0) continue;
+              T part = 0;
+#pragma unroll
+              for (int a = 0; a < K; ++a) {
+                T px, py, pz, pw;
+                target(a, px, py, pz, pw);
+                part += pw * (c < NS ? sl[c][a] : dl[a]);
+              }
+              if constexpr (F32) two_sum_add(acc_hi[c], acc_lo[c], part);
+              else acc_hi[c] += part;
+            }
           }
           g0 = g1;
         }
@@ -289,9 +309,14 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
     if (active) {
       const size_t stride = (size_t)md.nsplit * md.nitems;
       double* out = md.partial + (size_t)w.split * md.nitems + ti;
+      if constexpr (P1T) {
 #pragma unroll
-      for (int c = 0; c < NSL; ++c) out[c * stride] = (double)acc_hi[c] + (double)acc_lo[c];
-      if (DL) out[NSL * stride] = (double)acc_hi[NS] + (double)acc_lo[NS];
+        for (int k = 0; k < 3; ++k) out[k * stride] = (double)acc_hi[k] + (double)acc_lo[k];
+      } else {
+#pragma unroll
+        for (int c = 0; c < NSL; ++c) out[c * stride] = (double)acc_hi[c] + (double)acc_lo[c];
+        if (DL) out[NSL * stride] = (double)acc_hi[NS] + (double)acc_lo[NS];
+      }
     }
   }
 }
@@ -405,11 +430,11 @@ struct FarLaunch {
   bool DL;
 };
 
-template <typename T, int K, int NQ, int NSL, bool DL>
+template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
 static cudaError_t launch_far_t(const FarMeshDesc* d_meshes, const WorkItem* d_items, int nitems, int* d_counter,
                                 size_t smem, int grid, cudaStream_t st)
 {
-  auto kern = far_kernel<T, K, NQ, NSL, DL>;
+  auto kern = far_kernel<T, K, NQ, NSL, DL, P1T>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -418,58 +443,62 @@ static cudaError_t launch_far_t(const FarMeshDesc* d_meshes, const WorkItem* d_i
   return cudaGetLastError();
 }
 
-template <typename T, int K, int NQ, int NSL, bool DL>
+template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
 static int occupancy_t(size_t smem)
 {
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_kernel<T, K, NQ, NSL, DL>, kTT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_kernel<T, K, NQ, NSL, DL, P1T>, kTT, smem);
   return nb;
 }
 
-#define EB_FAR_CASES(X)                                                                                  \
-  X(1, 1) X(3, 3) X(4, 4) X(6, 6) X(7, 7) X(8, 0)
+// (points per item K, rule size NQ; NQ = 0: rule size read at run time)
+#define EB_FAR_CASES(X) X(1, 1) X(3, 3) X(4, 4) X(6, 6) X(7, 7) X(8, 0)
 
-// Operator variants compiled: (SL charges, DL).
+// Operator variants compiled: (SL charges, DL) for record preparation and
+// finalize; the far field adds the P1-test variant (1 charge, no DL).
 #define EB_VARIANTS(V) V(0, true) V(1, false) V(1, true) V(3, false) V(4, false)
+#define EB_FAR_VARIANTS(V) \
+  V(0, true, false) V(1, false, false) V(1, true, false) V(3, false, false) V(4, false, false) V(1, false, true)
 
-template <typename T, int NSL, bool DL>
+template <typename T, int NSL, bool DL, bool P1T>
 static cudaError_t dispatch_k(int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, size_t smem,
                               int grid, cudaStream_t st)
 {
-#define X(KK, NQQ) \
-  if (K == KK && (NQQ == 0 || Q == NQQ)) return launch_far_t<T, KK, NQQ, NSL, DL>(dm, di, n, dc, smem, grid, st);
+#define X(KK, NQQ)                                    \
+  if (K == KK && (NQQ == 0 || Q == NQQ))              \
+    return launch_far_t<T, KK, NQQ, NSL, DL, P1T>(dm, di, n, dc, smem, grid, st);
   EB_FAR_CASES(X)
 #undef X
   return cudaErrorInvalidValue;
 }
 
-template <typename T, int NSL, bool DL>
+template <typename T, int NSL, bool DL, bool P1T>
 static int dispatch_occ(int K, int Q, size_t smem)
 {
 #define X(KK, NQQ) \
-  if (K == KK && (NQQ == 0 || Q == NQQ)) return occupancy_t<T, KK, NQQ, NSL, DL>(smem);
+  if (K == KK && (NQQ == 0 || Q == NQQ)) return occupancy_t<T, KK, NQQ, NSL, DL, P1T>(smem);
   EB_FAR_CASES(X)
 #undef X
   return 0;
 }
 
 template <typename T>
-static cudaError_t far_launch_t(int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
-                                int* dc, size_t smem, int grid, cudaStream_t st)
+static cudaError_t far_launch_t(int NSL, bool DL, bool P1, int K, int Q, const FarMeshDesc* dm, const WorkItem* di,
+                                int n, int* dc, size_t smem, int grid, cudaStream_t st)
 {
-#define V(NS, D) \
-  if (NSL == NS && DL == D) return dispatch_k<T, NS, D>(K, Q, dm, di, n, dc, smem, grid, st);
-  EB_VARIANTS(V)
+#define V(NS, D, P) \
+  if (NSL == NS && DL == D && P1 == P) return dispatch_k<T, NS, D, P>(K, Q, dm, di, n, dc, smem, grid, st);
+  EB_FAR_VARIANTS(V)
 #undef V
   return cudaErrorInvalidValue;
 }
 
 template <typename T>
-static int far_occ_t(int NSL, bool DL, int K, int Q, size_t smem)
+static int far_occ_t(int NSL, bool DL, bool P1, int K, int Q, size_t smem)
 {
-#define V(NS, D) \
-  if (NSL == NS && DL == D) return dispatch_occ<T, NS, D>(K, Q, smem);
-  EB_VARIANTS(V)
+#define V(NS, D, P) \
+  if (NSL == NS && DL == D && P1 == P) return dispatch_occ<T, NS, D, P>(K, Q, smem);
+  EB_FAR_VARIANTS(V)
 #undef V
   return 0;
 }
@@ -484,15 +513,15 @@ bool far_variant_supported(int NSL, bool DL)
 }
 
 cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
-                       int* dc, size_t smem, int grid, cudaStream_t st)
+                       int* dc, size_t smem, int grid, cudaStream_t st, bool p1t)
 {
-  return fp32 ? far_launch_t<float>(NSL, DL, K, Q, dm, di, n, dc, smem, grid, st)
-              : far_launch_t<double>(NSL, DL, K, Q, dm, di, n, dc, smem, grid, st);
+  return fp32 ? far_launch_t<float>(NSL, DL, p1t, K, Q, dm, di, n, dc, smem, grid, st)
+              : far_launch_t<double>(NSL, DL, p1t, K, Q, dm, di, n, dc, smem, grid, st);
 }
 
-int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem)
+int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem, bool p1t)
 {
-  return fp32 ? far_occ_t<float>(NSL, DL, K, Q, smem) : far_occ_t<double>(NSL, DL, K, Q, smem);
+  return fp32 ? far_occ_t<float>(NSL, DL, p1t, K, Q, smem) : far_occ_t<double>(NSL, DL, p1t, K, Q, smem);
 }
 
 template <typename T>

@@ -64,6 +64,8 @@ constexpr double kFarRatio = 2.5;
 struct FarMeshDesc {
   const float4* tgt32;  // [nitems*K]: (x_a - centroid) in FP32, weight w_a
   const dq* tgt64;      // [nitems*K]: (x_a - centroid) in FP64, weight w_a
+  const float4* tgtw32; // [nitems*K]: w_a * (phi_0, phi_1, phi_2)(x_a), P1 test weights (FP32)
+  const dq* tgtw64;     // [nitems*K]: the same in FP64
   const dq* tcent;      // [nitems]: centroid of the item's triangle (FP64)
   const dq* tnrm;       // [nitems]: unit normal of the item's triangle (FP64)
   const dq* snrm;       // [ne]: unit normal n_j and plane offset P0_j . n_j of sorted sources

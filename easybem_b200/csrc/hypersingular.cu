@@ -66,9 +66,30 @@ __global__ void curl_scatter_kernel(int nv, int ne, const int* __restrict__ vptr
   out[a] = acc;
 }
 
+int ensure_vertex_lists(Mesh* m)
+{
+  if (m->vtri_ptr.p) return EB_OK;
+  const HostMesh& h = m->h;
+  // vertex -> (triangle, local index) in ascending triangle order
+  std::vector<int> vptr(h.nv + 1, 0), vlist(3 * (size_t)h.ne);
+  for (int e = 0; e < 3 * h.ne; e++) vptr[h.elems[e] + 1]++;
+  for (int v = 0; v < h.nv; v++) vptr[v + 1] += vptr[v];
+  std::vector<int> fill(vptr.begin(), vptr.end() - 1);
+  for (int i = 0; i < h.ne; i++)
+    for (int k = 0; k < 3; k++) vlist[fill[h.elems[3 * i + k]]++] = (i << 2) | k;
+  EB_CHECK(m->vtri_ptr.alloc(sizeof(int) * vptr.size()));
+  EB_CUDA(cudaMemcpy(m->vtri_ptr.p, vptr.data(), sizeof(int) * vptr.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(m->vtri_list.alloc(sizeof(int) * vlist.size()));
+  EB_CUDA(cudaMemcpy(m->vtri_list.p, vlist.data(), sizeof(int) * vlist.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(m->elems0.alloc(sizeof(int) * h.elems.size()));
+  EB_CUDA(cudaMemcpy(m->elems0.p, h.elems.data(), sizeof(int) * h.elems.size(), cudaMemcpyHostToDevice));
+  return EB_OK;
+}
+
 static int ensure_curls(Mesh* m)
 {
   if (m->curl9.p) return EB_OK;
+  EB_CHECK(ensure_vertex_lists(m));
   const HostMesh& h = m->h;
   std::vector<double> curl(9 * (size_t)h.ne);
   for (int i = 0; i < h.ne; i++) {
@@ -77,21 +98,8 @@ static int ensure_curls(Mesh* m)
     for (int k = 0; k < 3; k++) P[k] = mk3(h.nodes[3 * f[k]], h.nodes[3 * f[k] + 1], h.nodes[3 * f[k] + 2]);
     triangle_curls(P[0], P[1], P[2], &curl[9 * (size_t)i]);
   }
-  // vertex -> (triangle, local index) in ascending triangle order
-  std::vector<int> vptr(h.nv + 1, 0), vlist(3 * (size_t)h.ne);
-  for (int e = 0; e < 3 * h.ne; e++) vptr[h.elems[e] + 1]++;
-  for (int v = 0; v < h.nv; v++) vptr[v + 1] += vptr[v];
-  std::vector<int> fill(vptr.begin(), vptr.end() - 1);
-  for (int i = 0; i < h.ne; i++)
-    for (int k = 0; k < 3; k++) vlist[fill[h.elems[3 * i + k]]++] = (i << 2) | k;
   EB_CHECK(m->curl9.alloc(sizeof(double) * curl.size()));
   EB_CUDA(cudaMemcpy(m->curl9.p, curl.data(), sizeof(double) * curl.size(), cudaMemcpyHostToDevice));
-  EB_CHECK(m->vtri_ptr.alloc(sizeof(int) * vptr.size()));
-  EB_CUDA(cudaMemcpy(m->vtri_ptr.p, vptr.data(), sizeof(int) * vptr.size(), cudaMemcpyHostToDevice));
-  EB_CHECK(m->vtri_list.alloc(sizeof(int) * vlist.size()));
-  EB_CUDA(cudaMemcpy(m->vtri_list.p, vlist.data(), sizeof(int) * vlist.size(), cudaMemcpyHostToDevice));
-  EB_CHECK(m->elems0.alloc(sizeof(int) * h.elems.size()));
-  EB_CUDA(cudaMemcpy(m->elems0.p, h.elems.data(), sizeof(int) * h.elems.size(), cudaMemcpyHostToDevice));
   EB_CHECK(m->hs_x.alloc(sizeof(double) * 3 * (size_t)h.ne));
   EB_CHECK(m->hs_w.alloc(sizeof(double) * 3 * (size_t)h.ne));
   return EB_OK;

@@ -227,6 +227,120 @@ __device__ inline void near_pair_values(const Quadrature& q, const PairGeom& g, 
   }
 }
 
+// ---- P1 x P1 single layer: the reference GPU kernels' Sauter-Schwab forms
+// (src/BEM3dLaplaceGPU.cu:82-154, 211-320, 371-442, 491-557) in FP64.
+// I[3k+l] couples test basis k and trial basis l in the case's local vertex
+// order (p1_local_orders).
+
+__device__ inline void ss_p1_self(const Quadrature& q, d3 u, d3 v, double* I)
+{
+  double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const d3 uv = u + v;
+  for (int i = 0; i < q.nl; i++) {
+    const double e = q.lx[i], w = q.lw[i], e2 = e * e;
+    double f = w * rnorm(e * u + v);  // D1
+    S[0] += f / 30; S[1] += f / 60; S[2] += f / 30; S[3] += f / 60; S[4] += f / 30;
+    S[5] += f / 30; S[6] += f / 30; S[7] += f / 30; S[8] += f / 10;
+    f = w * rnorm(e * v + u);  // D2
+    S[0] += f / 30; S[1] += (2 - e) / 60 * f; S[2] += (1 + e) / 60 * f; S[3] += (2 - e) / 60 * f;
+    S[4] += (3 - 3 * e + e2) / 30 * f; S[5] += (1 + e - e2) / 30 * f; S[6] += (1 + e) / 60 * f;
+    S[7] += (1 + e - e2) / 30 * f; S[8] += (1 + e + e2) / 30 * f;
+    f = w * rnorm(e * uv - v);  // D3
+    S[0] += (1 + e + e2) / 30 * f; S[1] += (1 + e) / 60 * f; S[2] += (1 + e - e2) / 30 * f;
+    S[3] += (1 + e) / 60 * f; S[4] += f / 30; S[5] += (2 - e) / 60 * f;
+    S[6] += (1 + e - e2) / 30 * f; S[7] += (2 - e) / 60 * f; S[8] += (3 - 3 * e + e2) / 30 * f;
+  }
+  const d3 c = cross3(u, v);
+  const double sc = dot3(c, c) / (4.0 * M_PI);
+  for (int k = 0; k < 9; k++) I[k] = sc * S[k];
+}
+
+__device__ inline void ss_p1_edge(const Quadrature& q, d3 u, d3 v, d3 w, double* I)
+{
+  double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const d3 uw = u + w, uv = u + v;
+  for (int i = 0; i < q.nl; i++)
+    for (int j = 0; j < q.nl; j++) {
+      const double a = q.lx[i], b = q.lx[j], ww = q.lw[i] * q.lw[j], ab = a * b;
+      double f = ww * a * rnorm(a * (b * uw - w) + v);  // D2
+      S[0] += (1 + ab) / 60 * f; S[1] += (3 - 2 * a) / 120 * f; S[2] += -a * (b - 1) / 60 * f;
+      S[3] += (1 + 2 * ab) / 120 * f; S[4] += (2 - a) / 60 * f; S[5] += -a * (b - 1) / 60 * f;
+      S[6] += (1 + 3 * ab) / 60 * f; S[7] += (4 - 3 * a) / 60 * f; S[8] += -a * (b - 1) / 20 * f;
+      f = ww * a * rnorm(v - a * (uv + b * w));  // D3
+      S[0] += (1 + a) / 60 * f; S[1] += (1.0 / 40 + (4 * a - ab - 3 * a * ab) / 60) * f;
+      S[2] += ab * (3 * a + 1) / 60 * f; S[3] += f / 120; S[4] += (2 - ab) / 60 * f; S[5] += ab / 60 * f;
+      S[6] += (1 - a) / 60 * f; S[7] += (3 * ab - 4) * (a - 1) / 60 * f; S[8] += -ab * (a - 1) / 20 * f;
+      f = ww * a * rnorm(a * (v - b * uv) - w);  // D4
+      S[0] += (1 + ab) / 60 * f; S[1] += (1 + 2 * ab) / 120 * f; S[2] += (1 + 3 * ab) / 60 * f;
+      S[3] += (3 - 2 * a) / 120 * f; S[4] += (2 - a) / 60 * f; S[5] += (4 - 3 * a) / 60 * f;
+      S[6] += -a * (b - 1) / 60 * f; S[7] += -a * (b - 1) / 60 * f; S[8] += -a * (b - 1) / 20 * f;
+      f = ww * a * rnorm(v - a * (w + b * uv));  // D5
+      S[0] += (1 + ab) / 60 * f; S[1] += (1.0 / 40 + (4 * ab - a - 3 * a * ab) / 60) * f;
+      S[2] += a * (1 + 3 * ab) / 60 * f; S[3] += f / 120; S[4] += (2 - a) / 60 * f; S[5] += a / 60 * f;
+      S[6] += (1 - ab) / 60 * f; S[7] += (3 * a - 4) * (ab - 1) / 60 * f; S[8] += -a * (ab - 1) / 20 * f;
+      f = ww * rnorm(a * uw + b * v - w);  // D1
+      S[0] += (1 + a) / 60 * f; S[1] += f / 120; S[2] += (1 - a) / 60 * f;
+      S[3] += (1.0 / 40 + (4 * a - 3 * ab - b) / 60) * f; S[4] += (2 - b) / 60 * f;
+      S[5] += (3 * b - 4) * (a - 1) / 60 * f; S[6] += b * (3 * a + 1) / 60 * f; S[7] += b / 60 * f;
+      S[8] += -b * (a - 1) / 20 * f;
+    }
+  const double sc = sqrt(dot3(cross3(u, v), cross3(u, v))) * sqrt(dot3(cross3(u, w), cross3(u, w))) / (4.0 * M_PI);
+  for (int k = 0; k < 9; k++) I[k] = sc * S[k];
+}
+
+__device__ inline void ss_p1_vertex(const Quadrature& q, d3 u, d3 v, d3 w, d3 z, double* I)
+{
+  double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < q.nl; i++)
+    for (int j = 0; j < q.nl; j++)
+      for (int k = 0; k < q.nl; k++) {
+        const double e1 = q.lx[i], e2 = q.lx[j], e3 = q.lx[k];
+        const double ww = q.lw[i] * q.lw[j] * q.lw[k] * e2;
+        const double a[9] = {1.0 / 12 - e2 / 20,          e2 * e3 / 20,           -e2 * (e3 - 1) / 20,
+                             -e1 * (4 * e2 - 5) / 20,     e1 * e2 * e3 / 5,       -e1 * e2 * (e3 - 1) / 5,
+                             (4 * e2 - 5) * (e1 - 1) / 20, -e2 * e3 * (e1 - 1) / 5, e2 * (e1 - 1) * (e3 - 1) / 5};
+        const double f1 = ww * rnorm(u + e1 * v - e2 * (w + e3 * z));
+        const double f2 = ww * rnorm(w + e1 * z - e2 * (u + e3 * v));
+        for (int r = 0; r < 3; r++)
+          for (int c = 0; c < 3; c++) S[3 * r + c] += a[3 * r + c] * f1 + a[3 * c + r] * f2;
+      }
+  const double sc = sqrt(dot3(cross3(u, v), cross3(u, v))) * sqrt(dot3(cross3(w, z), cross3(w, z))) / (4.0 * M_PI);
+  for (int k = 0; k < 9; k++) I[k] = sc * S[k];
+}
+
+// P1 entries of a near pair; oi/oj: local vertex orders (p1_local_orders).
+__device__ inline void near_pair_values_p1(const Quadrature& q, const PairGeom& g, const d3* Pi, const d3* Pj,
+                                           const int* oi, const int* oj, double* I)
+{
+  if (g.kind == kPairSelf) {
+    ss_p1_self(q, Pi[1] - Pi[0], Pi[2] - Pi[1], I);
+  } else if (g.kind == kPairVertex) {
+    ss_p1_vertex(q, Pi[oi[1]] - Pi[oi[0]], Pi[oi[2]] - Pi[oi[1]], Pj[oj[1]] - Pj[oj[0]], Pj[oj[2]] - Pj[oj[1]], I);
+  } else if (g.kind == kPairEdge) {
+    ss_p1_edge(q, Pj[g.cj[1]] - Pj[g.cj[0]], Pi[g.ri] - Pj[g.cj[1]], Pj[g.rj] - Pj[g.cj[1]], I);
+  } else {
+    for (int k = 0; k < 9; k++) I[k] = 0.0;
+  }
+}
+
 #endif  // __CUDACC__
+
+// Local vertex orders of the test (oi) and trial (oj) basis functions of the
+// P1 near-pair formulas: coincident (0,1,2); vertex-adjacent rotations starting
+// at the shared vertex; edge-adjacent (shared c0, shared c1, opposite) in both
+// triangles (the reference GPU host code's P1..P3 / Q1..Q3, :1067-1083).
+__host__ __device__ inline void p1_local_orders(const PairGeom& g, int* oi, int* oj)
+{
+  for (int k = 0; k < 3; k++) oi[k] = oj[k] = k;
+  if (g.kind == kPairVertex) {
+    for (int k = 0; k < 3; k++) {
+      oi[k] = (g.ci[0] + k) % 3;
+      oj[k] = (g.cj[0] + k) % 3;
+    }
+  } else if (g.kind == kPairEdge) {
+    oi[0] = g.ci[0]; oi[1] = g.ci[1]; oi[2] = g.ri;
+    oj[0] = g.cj[0]; oj[1] = g.cj[1]; oj[2] = g.rj;
+  }
+}
 
 }  // namespace eb

@@ -1,0 +1,162 @@
+// Potential evaluation off the surface: u(x) = V t - W u (the representation
+// formula), as evaluateLaplace3d computes it (src/BEM3dLaplace.cpp:784-843):
+//
+//   u(x) = sum_j J_j/(4 pi) sum_b w_b [ t_j / |x - y_b| - u_h(y_b) (x - y_b).n_j / |x - y_b|^3 ]
+//
+// with the triangle rule of the mesh's quadrature index. Each thread owns one
+// evaluation point; a block takes 128 points and one chunk of source cells
+// staged through shared memory; per-chunk partial sums are added in a fixed
+// order by a second kernel (deterministic). The source records are the ones
+// the SL+DL apply prepares (charges w_b J_j t_j and strengths w_b J_j u_h);
+// (x - y).n_j is the signed distance of x from the plane of triangle j. FP32
+// evaluates cell-relative coordinates with per-cell two-sum accumulation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+#include <vector>
+
+#include "engine.h"
+
+namespace eb {
+
+constexpr int kPotThreads = 128;
+
+__device__ __forceinline__ void pot_two_sum(float& s, float& e, float x)
+{
+  const float t = __fadd_rn(s, x);
+  const float bp = __fsub_rn(t, s);
+  e = __fadd_rn(e, __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(x, bp)));
+  s = t;
+}
+
+template <typename T>
+struct PotSlot;
+template <>
+struct PotSlot<float> {
+  using type = float4;
+};
+template <>
+struct PotSlot<double> {
+  using type = dq;
+};
+
+__device__ __forceinline__ float pot_rsq(float x)
+{
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double pot_rsq(double x) { return rsqrt(x); }
+
+// records: 2 slots per source point, slot0 = (-2 y_rel, |y_rel|^2), slot1 = (s, c, ., .)
+template <typename T>
+__global__ void __launch_bounds__(kPotThreads) potential_kernel(int npts, const double* __restrict__ pts, int ne,
+                                                                int Q, int cells_per_chunk,
+                                                                const typename PotSlot<T>::type* __restrict__ rec,
+                                                                const typename PotSlot<T>::type* __restrict__ plane,
+                                                                const dq* __restrict__ ccent,
+                                                                double* __restrict__ partial)
+{
+  using S = typename PotSlot<T>::type;
+  constexpr bool F32 = std::is_same<T, float>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* s_rec = reinterpret_cast<S*>(smem_raw);
+  __shared__ S s_plane[kTS];
+  const int i = blockIdx.x * kPotThreads + threadIdx.x;
+  const bool active = i < npts;
+  const double px = active ? pts[3 * i] : 0.0, py = active ? pts[3 * i + 1] : 0.0, pz = active ? pts[3 * i + 2] : 0.0;
+  const int ncells = (ne + kCell - 1) / kCell;
+  const int c0 = blockIdx.y * cells_per_chunk, c1 = min(ncells, c0 + cells_per_chunk);
+  const int sb = c0 * kCell, se = min(ne, c1 * kCell);
+  T hi = 0, lo = 0;
+  for (int t0 = sb; t0 < se; t0 += kTS) {
+    const int ns = min(kTS, se - t0);
+    for (int k = threadIdx.x; k < ns * Q * 2; k += kPotThreads) s_rec[k] = rec[(size_t)t0 * Q * 2 + k];
+    for (int k = threadIdx.x; k < ns; k += kPotThreads) s_plane[k] = plane[t0 + k];
+    __syncthreads();
+    if (active) {
+      for (int g0 = 0; g0 < ns;) {
+        const int cell = (t0 + g0) / kCell;
+        const int g1 = min(ns, (cell + 1) * kCell - t0);
+        const dq cc = ccent[cell];
+        const T xs = (T)(px - cc.x), ys = (T)(py - cc.y), zs = (T)(pz - cc.z);
+        T part = 0;
+        for (int s = g0; s < g1; ++s) {
+          const S pn = s_plane[s];
+          const T d = xs * pn.x + (ys * pn.y + (zs * pn.z - pn.w));
+          T sl = 0, acc = 0;
+          const S* r = s_rec + (size_t)s * Q * 2;
+          for (int b = 0; b < Q; ++b) {
+            const S p0 = r[2 * b], p1 = r[2 * b + 1];
+            const T dx = xs + T(0.5) * p0.x, dy = ys + T(0.5) * p0.y, dz = zs + T(0.5) * p0.z;
+            const T inv = pot_rsq(dx * dx + dy * dy + dz * dz);
+            sl += p1.y * inv;
+            acc += (inv * inv) * (p1.x * inv);
+          }
+          part += sl - d * acc;
+        }
+        if constexpr (F32) pot_two_sum(hi, lo, part);
+        else hi += part;
+        g0 = g1;
+      }
+    }
+    __syncthreads();
+  }
+  if (active) partial[(size_t)blockIdx.y * npts + i] = (double)hi + (double)lo;
+}
+
+__global__ void potential_reduce_kernel(int npts, int nchunk, const double* __restrict__ partial,
+                                        double* __restrict__ out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  double s = 0.0;
+  for (int c = 0; c < nchunk; c++) s += partial[(size_t)c * npts + i];
+  out[i] = s * (0.25 / M_PI);
+}
+
+int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pts, const double* d_t,
+                            const double* d_u, double* d_out, cudaStream_t st)
+{
+  const HostMesh& h = m->h;
+  const bool fp32 = precision == EB_PREC_MIXED;
+  if (precision != EB_PREC_MIXED && precision != EB_PREC_FP64)
+    return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
+  if (npts < 1) return EB_OK;
+  if (h.Q > 16) return set_error(EB_ERR_INVALID, "potential evaluation supports triangle rules of up to 16 points");
+  // source records of the fused SL+DL variant (slot1 = (s, c))
+  if (!m->rec.p) {
+    EB_CHECK(m->rec.alloc((size_t)h.ne * h.Q * kMaxRecSlots * sizeof(dq)));
+    EB_CHECK(m->partial.alloc(sizeof(double) * (size_t)kMaxOutputs * m->plan.nsplit * h.nitems));
+  }
+  const ApplyArgs A = mesh_apply_args(m, fp32, m->rec.p, nullptr, d_t, h.ne, d_u, nullptr, h.ne, nullptr);
+  EB_CUDA(prep_launch(fp32, 1, true, A, st));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+  const int pblocks = (npts + kPotThreads - 1) / kPotThreads;
+  int nchunk = std::max(1, std::min(h.ncells, (4 * nsm + pblocks - 1) / pblocks));
+  const int cells_per = (h.ncells + nchunk - 1) / nchunk;
+  nchunk = (h.ncells + cells_per - 1) / cells_per;
+  EB_CHECK(m->pot_partial.alloc(sizeof(double) * (size_t)nchunk * npts));
+  const size_t smem = (size_t)kTS * h.Q * 2 * (fp32 ? sizeof(float4) : sizeof(dq));
+  const dim3 grid(pblocks, nchunk);
+  if (fp32) {
+    auto k = potential_kernel<float>;
+    if (smem > 48 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, m->rec.as<float4>(),
+                                       m->splane32.as<float4>(), m->ccent.as<dq>(), m->pot_partial.as<double>());
+  } else {
+    auto k = potential_kernel<double>;
+    if (smem > 48 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, m->rec.as<dq>(), m->splane64.as<dq>(),
+                                       m->ccent.as<dq>(), m->pot_partial.as<double>());
+  }
+  EB_CUDA(cudaGetLastError());
+  potential_reduce_kernel<<<(npts + 255) / 256, 256, 0, st>>>(npts, nchunk, m->pot_partial.as<double>(), d_out);
+  EB_CUDA(cudaGetLastError());
+  return EB_OK;
+}
+
+}  // namespace eb

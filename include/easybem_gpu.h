@@ -81,8 +81,13 @@ int eb_apply_sl_dl_noalloc(eb_mesh mesh, int precision, const double* d_t, const
 
 /* v = V1 t, the single layer with P1 test and trial functions (t, v have
  * nnodes entries). Replaces applyGPULaplace3d1Layer(t, v, 1)
- * (src/BEM3dLaplaceGPU.cu:82-154, 211-320, 371-442, 491-557, host :1034-1313). */
+ * (src/BEM3dLaplaceGPU.cu:82-154, 211-320, 371-442, 491-557, host :1034-1313)
+ * with the same Sauter-Schwab formulas in FP64, but trial indices taken from
+ * the trial triangle (the reference scatters them onto the test triangle's
+ * vertices off the diagonal, :1128, :1219, :1311, and drops a -1 at :1125). */
 int eb_apply_sl_p1(eb_mesh mesh, int precision, const double* t, double* v);
+/* Device-pointer form of eb_apply_sl_p1 on a stream (asynchronous). */
+int eb_apply_sl_p1_device(eb_mesh mesh, int precision, const double* d_t, double* d_v, void* stream);
 /* q = D u, the hypersingular operator in the curl form
  * D = sum_k C_k^T V C_k of getLaplace3d (src/BEM3dLaplace.cpp:767-771); u, q
  * have nnodes entries. Replaces the empty applyGPULaplace3dHyperSing
@@ -91,6 +96,13 @@ int eb_apply_hypersingular(eb_mesh mesh, int precision, const double* u, double*
 /* Device-pointer form of eb_apply_hypersingular on a stream (asynchronous). */
 int eb_apply_hypersingular_device(eb_mesh mesh, int precision, const double* d_u, double* d_q,
                                   void* stream);
+
+/* u(x) = V t - W u at npts points off the surface (the representation formula
+ * with the triangle rule of the mesh's order, up to 16 points): pts [npts][3],
+ * t [nelems], u [nnodes], out [npts], host memory. Replaces evaluateLaplace3d
+ * (src/BEM3dLaplace.cpp:784-843). */
+int eb_evaluate_potential(eb_mesh mesh, int precision, int npts, const double* pts, const double* t,
+                          const double* u, double* out);
 
 /* ---- Batched apply (no counterpart in the reference): the P0 single layer
  * of many meshes, each with ncols (1..4) right-hand sides, in one persistent

@@ -360,3 +360,203 @@ void orc_dense(const double *nodes, int nv, int ne, const int *elems, double *V,
     }
   }
 }
+
+/* Potential of the single layer of t minus the double layer of u at points
+ * (u(x) = V t - W u, the representation formula): src/BEM3dLaplace.cpp:784-843.
+ * The triangle rule is the one set by orc_set_rules (index `order`). */
+void orc_evaluate(const double *nodes, int ne, const int *elems, int npts, const double *pts,
+                  const double *t, const double *u, double *out, int nthreads)
+{
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < npts; i++) {
+    v3 x = load(pts + 3 * i);
+    double acc = 0.0;
+    for (int j = 0; j < ne; j++) {
+      const int *f = elems + 3 * j;
+      v3 A = load(nodes + 3 * (f[0] - 1));
+      v3 a = sub(load(nodes + 3 * (f[1] - 1)), A), b = sub(load(nodes + 3 * (f[2] - 1)), A);
+      v3 nt = cross(a, b);
+      double J = norm(nt);
+      v3 n = scl(1.0 / J, nt);
+      double u0 = u[f[0] - 1], u1 = u[f[1] - 1], u2 = u[f[2] - 1];
+      double s = 0.0;
+      for (int k = 0; k < g_nt; k++) {
+        v3 d = sub(sub(sub(x, A), scl(g_tx[k], a)), scl(g_ty[k], b));
+        double r = norm(d);
+        double uh = u0 + (u1 - u0) * g_tx[k] + (u2 - u0) * g_ty[k];
+        s += g_tw[k] * (t[j] / r - uh * dot(d, n) / (r * r * r));
+      }
+      acc += J * s / 4.0 / M_PI;
+    }
+    out[i] = acc;
+  }
+}
+
+/* ---- P1 x P1 single layer (no CPU routine in the reference). Restates the
+ * reference GPU kernels' Sauter-Schwab formulas in FP64:
+ * singleLayer1Laplace3d_idPanels (src/BEM3dLaplaceGPU.cu:82-154),
+ * _commonEdge (:211-320), _commonVertex (:371-442), _disjointPanels (:491-557).
+ * I[k][l] couples test basis k and trial basis l in each kernel's local vertex
+ * order; the host scatter of the reference (:1034-1313) uses the test
+ * triangle's vertices for the trial index off the diagonal, which is fixed
+ * here (trial indices come from the trial triangle). */
+static void p1_self(v3 u, v3 v, double I[3][3])
+{
+  double S[3][3] = {{0}};
+  for (int i = 0; i < g_nl; i++) {
+    double e = g_lx[i], w = g_lw[i], e2 = e * e, f;
+    f = w * inv_norm(add(scl(e, u), v)); /* D1 */
+    S[0][0] += f / 30; S[0][1] += f / 60; S[0][2] += f / 30; S[1][0] += f / 60; S[1][1] += f / 30;
+    S[1][2] += f / 30; S[2][0] += f / 30; S[2][1] += f / 30; S[2][2] += f / 10;
+    f = w * inv_norm(add(scl(e, v), u)); /* D2 */
+    S[0][0] += f / 30; S[0][1] += (2 - e) / 60 * f; S[0][2] += (1 + e) / 60 * f; S[1][0] += (2 - e) / 60 * f;
+    S[1][1] += (3 - 3 * e + e2) / 30 * f; S[1][2] += (1 + e - e2) / 30 * f; S[2][0] += (1 + e) / 60 * f;
+    S[2][1] += (1 + e - e2) / 30 * f; S[2][2] += (1 + e + e2) / 30 * f;
+    f = w * inv_norm(sub(scl(e, add(u, v)), v)); /* D3 */
+    S[0][0] += (1 + e + e2) / 30 * f; S[0][1] += (1 + e) / 60 * f; S[0][2] += (1 + e - e2) / 30 * f;
+    S[1][0] += (1 + e) / 60 * f; S[1][1] += f / 30; S[1][2] += (2 - e) / 60 * f;
+    S[2][0] += (1 + e - e2) / 30 * f; S[2][1] += (2 - e) / 60 * f; S[2][2] += (3 - 3 * e + e2) / 30 * f;
+  }
+  v3 c = cross(u, v);
+  double s = dot(c, c) / 4.0 / M_PI;
+  for (int k = 0; k < 3; k++)
+    for (int l = 0; l < 3; l++) I[k][l] = s * S[k][l];
+}
+
+static void p1_edge(v3 u, v3 v, v3 w, double I[3][3])
+{
+  double S[3][3] = {{0}};
+  v3 uw = add(u, w), uv = add(u, v);
+  for (int i = 0; i < g_nl; i++)
+    for (int j = 0; j < g_nl; j++) {
+      double a = g_lx[i], b = g_lx[j], ww = g_lw[i] * g_lw[j], ab = a * b, f;
+      f = ww * a * inv_norm(add(scl(a, sub(scl(b, uw), w)), v)); /* D2 */
+      S[0][0] += (1 + ab) / 60 * f; S[0][1] += (3 - 2 * a) / 120 * f; S[0][2] += -a * (b - 1) / 60 * f;
+      S[1][0] += (1 + 2 * ab) / 120 * f; S[1][1] += (2 - a) / 60 * f; S[1][2] += -a * (b - 1) / 60 * f;
+      S[2][0] += (1 + 3 * ab) / 60 * f; S[2][1] += (4 - 3 * a) / 60 * f; S[2][2] += -a * (b - 1) / 20 * f;
+      f = ww * a * inv_norm(add(scl(-a, add(uv, scl(b, w))), v)); /* D3 */
+      S[0][0] += (1 + a) / 60 * f; S[0][1] += (1.0 / 40 + (4 * a - ab - 3 * a * ab) / 60) * f;
+      S[0][2] += ab * (3 * a + 1) / 60 * f; S[1][0] += f / 120; S[1][1] += (2 - ab) / 60 * f;
+      S[1][2] += ab / 60 * f; S[2][0] += (1 - a) / 60 * f; S[2][1] += (3 * ab - 4) * (a - 1) / 60 * f;
+      S[2][2] += -ab * (a - 1) / 20 * f;
+      f = ww * a * inv_norm(sub(scl(a, sub(v, scl(b, uv))), w)); /* D4 */
+      S[0][0] += (1 + ab) / 60 * f; S[0][1] += (1 + 2 * ab) / 120 * f; S[0][2] += (1 + 3 * ab) / 60 * f;
+      S[1][0] += (3 - 2 * a) / 120 * f; S[1][1] += (2 - a) / 60 * f; S[1][2] += (4 - 3 * a) / 60 * f;
+      S[2][0] += -a * (b - 1) / 60 * f; S[2][1] += -a * (b - 1) / 60 * f; S[2][2] += -a * (b - 1) / 20 * f;
+      f = ww * a * inv_norm(add(scl(-a, add(w, scl(b, uv))), v)); /* D5 */
+      S[0][0] += (1 + ab) / 60 * f; S[0][1] += (1.0 / 40 + (4 * ab - a - 3 * a * ab) / 60) * f;
+      S[0][2] += a * (1 + 3 * ab) / 60 * f; S[1][0] += f / 120; S[1][1] += (2 - a) / 60 * f;
+      S[1][2] += a / 60 * f; S[2][0] += (1 - ab) / 60 * f; S[2][1] += (3 * a - 4) * (ab - 1) / 60 * f;
+      S[2][2] += -a * (ab - 1) / 20 * f;
+      f = ww * inv_norm(sub(add(scl(a, uw), scl(b, v)), w)); /* D1 */
+      S[0][0] += (1 + a) / 60 * f; S[0][1] += f / 120; S[0][2] += (1 - a) / 60 * f;
+      S[1][0] += (1.0 / 40 + (4 * a - 3 * ab - b) / 60) * f; S[1][1] += (2 - b) / 60 * f;
+      S[1][2] += (3 * b - 4) * (a - 1) / 60 * f; S[2][0] += b * (3 * a + 1) / 60 * f; S[2][1] += b / 60 * f;
+      S[2][2] += -b * (a - 1) / 20 * f;
+    }
+  double s = norm(cross(u, v)) * norm(cross(u, w)) / 4.0 / M_PI;
+  for (int k = 0; k < 3; k++)
+    for (int l = 0; l < 3; l++) I[k][l] = s * S[k][l];
+}
+
+static void p1_vertex(v3 u, v3 v, v3 w, v3 z, double I[3][3])
+{
+  double S[3][3] = {{0}};
+  for (int i = 0; i < g_nl; i++)
+    for (int j = 0; j < g_nl; j++)
+      for (int k = 0; k < g_nl; k++) {
+        double e1 = g_lx[i], e2 = g_lx[j], e3 = g_lx[k];
+        double ww = g_lw[i] * g_lw[j] * g_lw[k] * e2, f;
+        double a11 = 1.0 / 12 - e2 / 20, a12 = e2 * e3 / 20, a13 = -e2 * (e3 - 1) / 20;
+        double a21 = -e1 * (4 * e2 - 5) / 20, a22 = e1 * e2 * e3 / 5, a23 = -e1 * e2 * (e3 - 1) / 5;
+        double a31 = (4 * e2 - 5) * (e1 - 1) / 20, a32 = -e2 * e3 * (e1 - 1) / 5;
+        double a33 = e2 * (e1 - 1) * (e3 - 1) / 5;
+        f = ww * inv_norm(sub(add(u, scl(e1, v)), scl(e2, add(w, scl(e3, z)))));
+        S[0][0] += a11 * f; S[0][1] += a12 * f; S[0][2] += a13 * f; S[1][0] += a21 * f; S[1][1] += a22 * f;
+        S[1][2] += a23 * f; S[2][0] += a31 * f; S[2][1] += a32 * f; S[2][2] += a33 * f;
+        f = ww * inv_norm(sub(add(w, scl(e1, z)), scl(e2, add(u, scl(e3, v)))));
+        S[0][0] += a11 * f; S[1][0] += a12 * f; S[2][0] += a13 * f; S[0][1] += a21 * f; S[1][1] += a22 * f;
+        S[2][1] += a23 * f; S[0][2] += a31 * f; S[1][2] += a32 * f; S[2][2] += a33 * f;
+      }
+  double s = norm(cross(u, v)) * norm(cross(w, z)) / 4.0 / M_PI;
+  for (int k = 0; k < 3; k++)
+    for (int l = 0; l < 3; l++) I[k][l] = s * S[k][l];
+}
+
+static void p1_disjoint(v3 A, v3 u, v3 v, v3 B, v3 w, v3 z, double I[3][3])
+{
+  double S[3][3] = {{0}};
+  for (int i = 0; i < g_nt; i++) {
+    v3 x = add(A, add(scl(g_tx[i], u), scl(g_ty[i], v)));
+    double pi[3] = {1 - g_tx[i] - g_ty[i], g_tx[i], g_ty[i]};
+    for (int j = 0; j < g_nt; j++) {
+      v3 y = add(B, add(scl(g_tx[j], w), scl(g_ty[j], z)));
+      double f = g_tw[i] * g_tw[j] * inv_norm(sub(x, y));
+      double pj[3] = {1 - g_tx[j] - g_ty[j], g_tx[j], g_ty[j]};
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) S[k][l] += pi[k] * pj[l] * f;
+    }
+  }
+  double s = norm(cross(u, v)) * norm(cross(w, z)) / 4.0 / M_PI;
+  for (int k = 0; k < 3; k++)
+    for (int l = 0; l < 3; l++) I[k][l] = s * S[k][l];
+}
+
+/* P1 entries of pair (test i, trial j): I[k][l] couples vertex ti[k] (0-based)
+ * with vertex tj[l]. Returns 0 for a repeated triangle (nothing added). */
+int orc_p1_pair(const double *nodes, const int *elems, int i, int j, double *I9, int *ti, int *tj)
+{
+  const int *fi = elems + 3 * i, *fj = elems + 3 * j;
+  v3 Pi[3], Pj[3];
+  for (int k = 0; k < 3; k++) {
+    Pi[k] = load(nodes + 3 * (fi[k] - 1));
+    Pj[k] = load(nodes + 3 * (fj[k] - 1));
+  }
+  double I[3][3];
+  int oi[3] = {0, 1, 2}, oj[3] = {0, 1, 2};
+  if (i == j) {
+    p1_self(sub(Pi[1], Pi[0]), sub(Pi[2], Pi[1]), I);
+  } else {
+    int ci[2], cj[2], ri = 0, rj = 0;
+    int nc = classify(fi, fj, ci, cj, &ri, &rj);
+    if (nc == 0) {
+      p1_disjoint(Pi[0], sub(Pi[1], Pi[0]), sub(Pi[2], Pi[0]), Pj[0], sub(Pj[1], Pj[0]), sub(Pj[2], Pj[0]), I);
+    } else if (nc == 1) {
+      int p = ci[0], q = cj[0];
+      for (int k = 0; k < 3; k++) { oi[k] = (p + k) % 3; oj[k] = (q + k) % 3; }
+      p1_vertex(sub(Pi[oi[1]], Pi[oi[0]]), sub(Pi[oi[2]], Pi[oi[1]]), sub(Pj[oj[1]], Pj[oj[0]]),
+                sub(Pj[oj[2]], Pj[oj[1]]), I);
+    } else if (nc == 2) {
+      oi[0] = ci[0]; oi[1] = ci[1]; oi[2] = ri;
+      oj[0] = cj[0]; oj[1] = cj[1]; oj[2] = rj;
+      p1_edge(sub(Pj[cj[1]], Pj[cj[0]]), sub(Pi[ri], Pj[cj[1]]), sub(Pj[rj], Pj[cj[1]]), I);
+    } else {
+      return 0;
+    }
+  }
+  for (int k = 0; k < 3; k++) {
+    ti[k] = fi[oi[k]] - 1;
+    tj[k] = fj[oj[k]] - 1;
+    for (int l = 0; l < 3; l++) I9[3 * k + l] = I[k][l];
+  }
+  return 1;
+}
+
+/* Dense V1 (nv x nv), row = test vertex. */
+void orc_p1_dense(const double *nodes, int nv, int ne, const int *elems, double *V1)
+{
+  memset(V1, 0, sizeof(double) * (size_t)nv * nv);
+  for (int i = 0; i < ne; i++)
+    for (int j = 0; j < ne; j++) {
+      double I9[9];
+      int ti[3], tj[3];
+      if (!orc_p1_pair(nodes, elems, i, j, I9, ti, tj)) continue;
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) V1[(size_t)ti[k] * nv + tj[l]] += I9[3 * k + l];
+    }
+}

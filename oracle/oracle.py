@@ -133,6 +133,32 @@ class Oracle:
         self.lib.orc_dense(_d(nodes), nv, ne, _i(elems), _d(V), _d(K), nthreads)
         return V, K
 
+    def evaluate(self, nodes, elems, points, t, u, nthreads: int = 0):
+        """u(x) = V t - W u at points (the representation formula)."""
+        nodes, elems = self._mesh(nodes, elems)
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        out = np.zeros(pts.shape[0])
+        self.lib.orc_evaluate(_d(nodes), elems.shape[0], _i(elems), pts.shape[0], _d(pts),
+                              _d(np.ascontiguousarray(t, dtype=np.float64)),
+                              _d(np.ascontiguousarray(u, dtype=np.float64)), _d(out), nthreads)
+        return out
+
+    def p1_dense(self, nodes, elems):
+        """Dense P1 x P1 single layer (nv x nv, row = test vertex)."""
+        nodes, elems = self._mesh(nodes, elems)
+        nv = nodes.shape[0]
+        V1 = np.zeros((nv, nv))
+        self.lib.orc_p1_dense(_d(nodes), nv, elems.shape[0], _i(elems), _d(V1))
+        return V1
+
+    def p1_pair(self, nodes, elems, i, j):
+        nodes, elems = self._mesh(nodes, elems)
+        I9 = np.zeros(9)
+        ti = np.zeros(3, dtype=np.int32)
+        tj = np.zeros(3, dtype=np.int32)
+        ok = self.lib.orc_p1_pair(_d(nodes), _i(elems), int(i), int(j), _d(I9), _i(ti), _i(tj))
+        return bool(ok), I9.reshape(3, 3), ti, tj
+
     def pair(self, nodes, elems, i, j):
         nodes, elems = self._mesh(nodes, elems)
         vij = ctypes.c_double()
@@ -144,6 +170,19 @@ class Oracle:
 
 def ref_set_order(order: int):
     ref_lib().ref_set_order(order)
+
+
+def ref_evaluate(nodes, elems, points, t, u, order: int = 4):
+    """The reference's evaluateLaplace3d (src/BEM3dLaplace.cpp:784-843)."""
+    lib = ref_lib()
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    elems = np.ascontiguousarray(elems, dtype=np.int32)
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    out = np.zeros(pts.shape[0])
+    lib.ref_evaluate(_d(nodes), elems.shape[0], _i(elems), pts.shape[0], _d(pts),
+                     _d(np.ascontiguousarray(t, dtype=np.float64)), _d(np.ascontiguousarray(u, dtype=np.float64)),
+                     order, _d(out))
+    return out
 
 
 def ref_apply_rows(nodes, elems, t, u, rows=None, nthreads: int = 0, order: int = 4):

@@ -11,7 +11,7 @@ Writes
   src/quadrature.cpp;
 * ``reference_ops.npz``: dense getLaplace3d V, K, M (src/BEM3dLaplace.cpp:
   561-781) on small meshes, and V t, K u for seeded densities, at several
-  quadrature indices. The cube is the reference example mesh
+  quadrature indices, plus evaluateLaplace3d (:784-843) at seeded points. The cube is the reference example mesh
   python/examples/cube01-surface.txt (8 vertices, 12 triangles).
 """
 from __future__ import annotations
@@ -78,6 +78,16 @@ def main():
             if o == 4:
                 out[f"{name}_M1"] = M @ np.ones(nodes.shape[0])
                 out[f"{name}_Du"] = D @ u
+                # evaluateLaplace3d at points inside, outside and near the surface
+                c = nodes.mean(axis=0)
+                rad = np.max(np.linalg.norm(nodes - c, axis=1))
+                prng = np.random.default_rng(13)
+                dirs = prng.normal(size=(12, 3))
+                dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+                scale = np.array([0.1, 0.4, 1.6, 3.0] * 3)[:, None]
+                pts = c + dirs * rad * scale
+                out[f"{name}_pts"] = pts
+                out[f"{name}_eval"] = O.ref_evaluate(nodes, elems, pts, t, u, 4)
     np.savez_compressed(os.path.join(HERE, "reference_ops.npz"), **out)
     print("wrote", sorted(os.listdir(HERE)))
 

@@ -103,3 +103,29 @@ def test_reference_dense_equals_reference_matrix_free():
     v, q = O.ref_apply_rows(nodes, elems, t, u)
     assert rel_l2(V @ t, v) < 1e-14
     assert rel_l2(K @ u, q) < 1e-14
+
+
+def test_p1_single_layer_formulas_sum_to_pinned_p0(oracle):
+    # The P1 x P1 Sauter-Schwab formulas (restated from the reference GPU
+    # kernels; the reference has no CPU P1 single layer) must sum over the 9
+    # basis pairs to the P0 entry, which is pinned to the reference CPU code
+    # (partition of unity on both triangles). This also fixes the local
+    # test/trial vertex orders of every near-pair case.
+    nodes, elems = meshes.perturbed_icosphere(2, seed=3)
+    ne = elems.shape[0]
+    oracle.set_order(4)
+    checked = 0
+    for i in range(0, ne, 7):
+        for j in range(ne):
+            shared = len(set(elems[i]) & set(elems[j]))
+            if i != j and shared == 0 and (i + j) % 11:
+                continue
+            ok, I, ti, tj = oracle.p1_pair(nodes, elems, i, j)
+            vij, _, _ = oracle.pair(nodes, elems, i, j)
+            assert ok
+            assert abs(I.sum() - vij) <= 1e-13 * abs(vij)
+            checked += 1
+    assert checked > 200
+    V1 = oracle.p1_dense(nodes, elems)
+    assert np.linalg.norm(V1 - V1.T) / np.linalg.norm(V1) < 1e-6
+    assert np.linalg.eigvalsh(0.5 * (V1 + V1.T)).min() > 0
