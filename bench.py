@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--level", type=int, default=LEVEL)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="matvec: keep the default launch plan instead of tuning it on the mesh first")
     p.add_argument("--workload", default="matvec", choices=["matvec", "batch", "serve", "large", "small"],
                    help="matvec: the headline single-mesh SL+DL apply (default); batch: 256 uneven "
                         "ellipsoids x 4 RHS, batched apply and GMRES-IR solves; serve: Poisson stream of "
@@ -413,6 +415,12 @@ def main():
         ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
         return ms, far_ms
 
+    # launch plan: tuned on this mesh before any timing (untimed setup)
+    plan = None if args.no_autotune else mesh.autotune(precision="mixed", operators="sl+dl", reps=2)
+    plan_info = dict(mesh.plan(), tuned=plan is not None)
+    if plan is not None:
+        plan_info.update(tuned_ms=plan["ms"], default_ms=plan["start_ms"])
+
     # headline: mixed precision, device-resident inputs
     sampler = ClockSampler(local)
     ms_mixed, far_mixed = timed("mixed", args.steps, args.warmup, sampler)
@@ -492,7 +500,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 far field / f64 near field", "data": "synthetic",
         "config": {"workload": WORKLOAD.format(level=args.level, ne=ne, nv=nv), "triangles": ne, "vertices": nv, "quad_pairs_per_step": pairs,
-                   "near_pairs": mesh.near_pairs, "parallelism": f"replicas x{world}",
+                   "near_pairs": mesh.near_pairs, "parallelism": f"replicas x{world}", "plan": plan_info,
                    "l2": "flushed between timed steps (256 MB write)"},
         "fp64": {"value": value64, "unit": "Gpairs/s", "ms_per_step": step_ms64, "steps": len(ms_fp64),
                  "far_ms": sum(f for f, _ in far_fp64) / len(far_fp64)},

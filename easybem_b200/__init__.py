@@ -23,7 +23,7 @@ from ._lib import EB_PREC_FP64, EB_PREC_MIXED, EasyBemError, SolveOptions, Solve
 
 __all__ = ["Mesh", "Batch", "Solver", "Server", "solve", "EasyBemError", "init_gpu", "close_gpu", "apply_gpu_laplace3d_1layer",
            "apply_gpu_laplace3d_1layer_linears", "apply_gpu_laplace3d_2layer",
-           "apply_gpu_laplace3d_hypersing", "version", "precision_code"]
+           "apply_gpu_laplace3d_hypersing", "version", "precision_code", "save_plans", "load_plans", "clear_plans"]
 
 
 def precision_code(precision) -> int:
@@ -162,6 +162,43 @@ class Mesh:
         a, b = ctypes.c_double(), ctypes.c_double()
         check(lib().eb_last_kernel_ms(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    # launch plan -----------------------------------------------------------
+    def plan(self):
+        """The far-field launch plan: dict(items_per_sm, src_tile, nsplit, work_items)."""
+        a, b, c, d = (ctypes.c_int() for _ in range(4))
+        check(lib().eb_mesh_get_plan(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
+        return {"items_per_sm": a.value, "src_tile": b.value, "nsplit": c.value, "work_items": d.value}
+
+    def set_plan(self, items_per_sm: int = 32, src_tile: int = 0):
+        check(lib().eb_mesh_set_plan(self._h, int(items_per_sm), int(src_tile)))
+
+    def autotune(self, precision="mixed", operators="sl+dl", reps: int = 3):
+        """Times the candidate plans on this mesh and keeps the fastest.
+
+        Returns dict(items_per_sm, src_tile, ms, start_ms)."""
+        ops = {"sl": 1, "dl": 2, "sl+dl": 3}[operators]
+        a, b = ctypes.c_int(), ctypes.c_int()
+        ms, ms0 = ctypes.c_double(), ctypes.c_double()
+        check(lib().eb_autotune(self._h, precision_code(precision), ops, int(reps), ctypes.byref(a), ctypes.byref(b),
+                                ctypes.byref(ms), ctypes.byref(ms0)))
+        return {"items_per_sm": a.value, "src_tile": b.value, "ms": ms.value, "start_ms": ms0.value}
+
+
+def save_plans(path: str):
+    """Writes the process-wide table of tuned plans to a text file."""
+    check(lib().eb_plan_table_save(os.fsencode(path)))
+
+
+def load_plans(path: str) -> int:
+    """Merges a saved plan table; meshes created afterwards start from it."""
+    n = ctypes.c_int()
+    check(lib().eb_plan_table_load(os.fsencode(path), ctypes.byref(n)))
+    return n.value
+
+
+def clear_plans():
+    check(lib().eb_plan_table_clear())
 
 
 class Batch:

@@ -75,6 +75,15 @@ _SIGNATURES = {
     "eb_server_release": (ctypes.c_int, [_dp, ctypes.c_longlong]),
     "eb_server_usage": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "eb_last_kernel_ms": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "eb_mesh_set_plan": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int]),
+    "eb_mesh_get_plan": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "eb_autotune": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]),
+    "eb_plan_table_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "eb_plan_table_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
+    "eb_plan_table_clear": (ctypes.c_int, []),
 }
 
 

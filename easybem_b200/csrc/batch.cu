@@ -51,6 +51,8 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     Mesh* m = be->mesh;
     const HostMesh& h = m->h;
     if (h.Q != Q_) return set_error(EB_ERR_INVALID, "a batch needs one quadrature order for all meshes");
+    // the mesh's plan may have changed (finer work split) since the entry was made
+    EB_CHECK(be->partial.alloc(sizeof(double) * (size_t)kBatchCols * m->plan.nsplit * h.nitems));
     desc[e] = mesh_far_desc(m, fp32, nsl_, false, be->rec.p, be->partial.as<double>());
     desc[e].active = d_flags ? d_flags + e : nullptr;
     src_tile = std::min(src_tile, desc[e].src_tile);

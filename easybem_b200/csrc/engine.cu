@@ -262,7 +262,7 @@ static int build_items(Mesh* m)
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
   const int ntt = (h.nitems + kTT - 1) / kTT;
-  const int want = nsm * 32;  // work items for balance across persistent CTAs
+  const int want = nsm * std::max(1, m->plan.items_per_sm);  // work items for balance across persistent CTAs
   int nsplit = std::max(1, std::min(h.ncells, (want + ntt - 1) / ntt));
   const int cells_per = (h.ncells + nsplit - 1) / nsplit;
   nsplit = (h.ncells + cells_per - 1) / cells_per;
@@ -279,6 +279,23 @@ static int build_items(Mesh* m)
   return EB_OK;
 }
 
+int mesh_set_plan(Mesh* m, int items_per_sm, int tile)
+{
+  if (items_per_sm < 1 || items_per_sm > 4096 || tile < 0 || tile > kTS)
+    return set_error(EB_ERR_INVALID, "plan needs 1 <= items_per_sm <= 4096 and 0 <= tile <= " + std::to_string(kTS));
+  EB_CUDA(cudaDeviceSynchronize());
+  m->plan.items_per_sm = items_per_sm;
+  m->plan.tile = tile;
+  // per-variant descriptors and the scratch sized for the old split go away
+  for (auto& v : m->variants) {
+    v.desc.release();
+    v.grid = 0;
+  }
+  m->rec.release();
+  m->partial.release();
+  return build_items(m);
+}
+
 int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int order, Mesh** out)
 {
   int ndev = 0;
@@ -288,6 +305,7 @@ int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int orde
   Mesh* m = new Mesh();
   cudaGetDevice(&m->device);
   int st = prepare_host_mesh(nv, nodes, ne, elems1, order, &m->h);
+  if (st == EB_OK) tuned_plan_for(m->h, &m->plan.items_per_sm, &m->plan.tile);
   if (st == EB_OK) st = build_static(m);
   if (st == EB_OK) st = build_near(m);
   if (st == EB_OK) st = build_items(m);
@@ -358,6 +376,7 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec,
   desc.Q = h.Q;
   desc.nsplit = m->plan.nsplit;
   desc.src_tile = src_tile_for(h.Q, fp32, nsl, dl);
+  if (m->plan.tile > 0) desc.src_tile = std::min(desc.src_tile, m->plan.tile);
   desc.active = nullptr;
   return desc;
 }

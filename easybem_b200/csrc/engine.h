@@ -40,9 +40,11 @@ struct DevBuf {
 
 // Launch plan of the far field for one mesh (tile shape and work split).
 struct FarPlan {
-  int src_tile = kTS;  // source triangles per shared-memory tile
-  int nsplit = 1;      // source ranges per target tile
-  int grid = 0;        // persistent CTAs
+  int items_per_sm = 32;  // work items per SM the source ranges are cut into (load balance)
+  int tile = 0;           // source triangles per shared-memory tile (0: the variant's default)
+  int src_tile = kTS;     // tile of the last launch
+  int nsplit = 1;         // source ranges per target tile
+  int grid = 0;           // persistent CTAs of the last launch
   size_t smem = 0;
 };
 
@@ -102,6 +104,11 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
                             const double* d_u, double* d_out, cudaStream_t st);
 // v = V1 t, P1 x P1 single layer; t and v have nnodes entries (device).
 int mesh_apply_sl_p1(Mesh* m, int precision, const double* d_t, double* d_v, cudaStream_t st);
+// Replaces the launch plan (work split, source tile) of a mesh; later applies
+// and batches use it. Waits for the mesh's work to finish first.
+int mesh_set_plan(Mesh* m, int items_per_sm, int tile);
+// The tuned plan recorded for meshes like m (returns false if none).
+bool tuned_plan_for(const HostMesh& h, int* items_per_sm, int* tile);
 // vertex -> (triangle, local index) lists on the device (built on first use)
 int ensure_vertex_lists(Mesh* m);
 // q = D u (hypersingular, curl form); u and q have nnodes entries (device).

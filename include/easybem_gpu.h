@@ -215,6 +215,32 @@ int eb_measure_fp32_peak(double* tflops, double* seconds);
 int eb_set_profiling(eb_mesh mesh, int on);
 int eb_last_kernel_ms(eb_mesh mesh, double* far_ms, double* finalize_ms);
 
+/* Launch plan of a mesh's far field: work items per SM (how finely the source
+ * range of every 128-target tile is cut for the persistent CTAs' queue) and
+ * source triangles per shared-memory tile (0 = the variant's default, at most
+ * 64). eb_mesh_set_plan waits for the device, rebuilds the work list and drops
+ * the cached launch descriptors; batches and solvers built later use the new
+ * plan. Not to be called while another call on the same mesh runs. Results
+ * change only by rounding (summation order). No counterpart in the reference,
+ * whose launch shape is fixed (src/BEM3dLaplaceGPU.cu:985-1322, 256 threads). */
+int eb_mesh_set_plan(eb_mesh mesh, int items_per_sm, int src_tile);
+int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit, int* work_items);
+
+/* Times candidate plans (items_per_sm in {4,8,...,512} x source tile in
+ * {default, 32, 16}) on this mesh with CUDA events, median of `reps` applies
+ * each; operators: 1 = SL, 2 = DL, 3 = SL+DL. Keeps the fastest on the mesh
+ * and records it in the process-wide plan table under (SM count,
+ * floor(log2 nelems), triangle-rule points, precision); meshes created later
+ * that match an entry start from it (mixed entries first). start_ms is the
+ * time of the plan the mesh had. No counterpart in the reference. */
+int eb_autotune(eb_mesh mesh, int precision, int operators, int reps, int* items_per_sm, int* src_tile,
+                double* best_ms, double* start_ms);
+/* Plan table as text: a header line, then "sms bucket points precision
+ * items_per_sm src_tile ms" per entry. Load merges into the table. */
+int eb_plan_table_save(const char* path);
+int eb_plan_table_load(const char* path, int* loaded);
+int eb_plan_table_clear(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -115,3 +115,27 @@ def test_mesh_create_without_gpu_fails_loudly():
     v, f = meshes.icosphere(1)
     with pytest.raises(EasyBemError):
         Mesh(v, f)
+
+
+def test_plan_table_file_round_trip(tmp_path):
+    # host-only: the table is plain text and needs no device
+    import easybem_b200 as eb
+    good = tmp_path / "plans.txt"
+    good.write_text("easybem-b200-plans 1\n148 16 7 1 16 0 12.5\n148 12 7 0 64 32 0.75\n")
+    eb.clear_plans()
+    assert eb.load_plans(str(good)) == 2
+    out = tmp_path / "saved.txt"
+    eb.save_plans(str(out))
+    lines = out.read_text().splitlines()
+    assert lines[0] == "easybem-b200-plans 1"
+    rows = sorted(tuple(float(x) for x in l.split()) for l in lines[1:])
+    assert rows == sorted([(148, 16, 7, 1, 16, 0, 12.5), (148, 12, 7, 0, 64, 32, 0.75)])
+    bad = tmp_path / "bad.txt"
+    for text in ("not a table\n", "easybem-b200-plans 1\n148 16 7 1 0 0 1.0\n",
+                 "easybem-b200-plans 1\n148 16 7 2 16 0 1.0\n", "easybem-b200-plans 1\n148 16 7 1 16 99 1.0\n"):
+        bad.write_text(text)
+        with pytest.raises(eb.EasyBemError):
+            eb.load_plans(str(bad))
+    with pytest.raises(eb.EasyBemError):
+        eb.load_plans(str(tmp_path / "missing.txt"))
+    eb.clear_plans()
