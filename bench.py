@@ -48,7 +48,7 @@ FLOPS_PER_PAIR = 20  # SL: 3 sub + 5 (|r|^2) + 1 rsqrt + 2 fma; DL: 5 (r.p) + 2 
 FAR_TRAFFIC_L6 = 39.64e6 + 0.76e6
 
 
-def parse():
+def parse_args(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=10)
@@ -66,7 +66,7 @@ def parse():
     p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
     p.add_argument("--serve-sample", type=int, default=32,
                    help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
-    return p.parse_args()
+    return p.parse_args(argv)
 
 
 def dist_env():
@@ -74,6 +74,22 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The largest value of x over all ranks (the slowest replica's time)."""
+    if dist is None:
+        return x
+    import torch
+    tt = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_throughput(world, pairs_per_replica, step_ms):
+    """Whole-job Gpairs/s of `world` independent replicas, each applying
+    `pairs_per_replica` pairs per step, timed by the slowest rank's step."""
+    return world * pairs_per_replica / (step_ms * 1e-3) / 1e9
 
 
 class ClockSampler:
@@ -354,7 +370,7 @@ def run_small(args):
 
 
 def main():
-    args = parse()
+    args = parse_args()
     if args.impl == "reference":
         run_reference(args)
         return
@@ -432,17 +448,10 @@ def main():
     v_64 = d_v.cpu().numpy()
     q_64 = d_q.cpu().numpy()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        tt = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
-
-    step_ms = max_over_ranks(sum(ms_mixed) / len(ms_mixed))
-    step_ms64 = max_over_ranks(sum(ms_fp64) / len(ms_fp64))
-    value = world * pairs / (step_ms * 1e-3) / 1e9
-    value64 = world * pairs / (step_ms64 * 1e-3) / 1e9
+    step_ms = max_over_ranks(sum(ms_mixed) / len(ms_mixed), dist, dev)
+    step_ms64 = max_over_ranks(sum(ms_fp64) / len(ms_fp64), dist, dev)
+    value = replica_throughput(world, pairs, step_ms)
+    value64 = replica_throughput(world, pairs, step_ms64)
 
     # e2e through the host-buffer C ABI with pinned host memory
     h_t = torch.from_numpy(t).pin_memory()
@@ -463,8 +472,8 @@ def main():
         _lib.check(L.eb_apply_sl_dl(mesh.handle, 1, P(h_t), P(h_u), P(h_v), P(h_q)))
         e2e_times.append(time.perf_counter() - a)
     barrier()
-    e2e_s = max_over_ranks(sum(e2e_times) / len(e2e_times))
-    e2e_value = world * pairs / e2e_s / 1e9
+    e2e_s = max_over_ranks(sum(e2e_times) / len(e2e_times), dist, dev)
+    e2e_value = replica_throughput(world, pairs, 1e3 * e2e_s)
 
     if rank != 0:
         if dist is not None:
