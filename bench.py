@@ -42,10 +42,16 @@ SEED = 1
 ORDER = 4
 WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L{level} "
             "({ne:,} triangles, {nv:,} vertices), quadrature index 4 (Q=7)")
-FLOPS_PER_PAIR = 20  # SL: 3 sub + 5 (|r|^2) + 1 rsqrt + 2 fma; DL: 5 (r.p) + 2 mul + 2 fma (FMA = 2)
+# Algorithmic FP32-pipe work of one far-cell quadrature pair of the fused SL+DL apply:
+# |x-y|^2 = |x|^2 + |y|^2 - 2x.y is 1 add + 3 FMA, the SL term 1 FMA, the DL term s/r^3 is
+# 2 mul + 1 FMA: 8 FMA-pipe operations, counted as 2 flops each (the unit of the FFMA peak),
+# plus 1 MUFU reciprocal square root. Both pipes bound the kernel.
+FMA_OPS_PER_PAIR = 8
+FLOPS_PER_PAIR = 2 * FMA_OPS_PER_PAIR
+RSQRT_PER_PAIR = 1
 # DRAM bytes (read + write) of one far-field launch on the L6 workload, from the ncu capture
-# summarised in profiles/far_kernel_f32_sl_dl_icosphere_L6.md (39.64 MB read + 0.76 MB written).
-FAR_TRAFFIC_L6 = 39.64e6 + 0.76e6
+# summarised in profiles/far_kernel_f32_sl_dl_icosphere_L6.md (39.70 MB read + 1.36 MB written).
+FAR_TRAFFIC_L6 = 39.70e6 + 1.36e6
 
 
 def parse_args(argv=None):
@@ -494,8 +500,12 @@ def main():
     # roofline of the dominant kernel (far field), event-timed on its stream
     far_avg = sum(f for f, _ in far_mixed) / len(far_mixed)
     fin_avg = sum(g for _, g in far_mixed) / len(far_mixed)
-    peak_tflops, _ = _measure_peak()
-    achieved = pairs * FLOPS_PER_PAIR / (far_avg * 1e-3) / 1e12
+    peak_tflops, peak_rsqrt = _measure_peak()
+    pair_rate = pairs / (far_avg * 1e-3)
+    achieved = pair_rate * FLOPS_PER_PAIR / 1e12
+    mufu = pair_rate * RSQRT_PER_PAIR / 1e12
+    # the pair rate both pipes allow together, and the fraction of it reached
+    pair_bound = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
     near_bytes = 12 * mesh.near_pairs + 8 * ne * 13 * 3  # SL CSR + DL CSR values/cols (approx.)
     cpu = None if args.no_cpu_baseline else cpu_reference_sample(nodes, elems, t, u)
     clocks = sampler.summary()
@@ -518,12 +528,16 @@ def main():
         "e2e": {"value": e2e_value, "unit": "Gpairs/s", "h2d_bytes_per_step": 8 * (ne + nv),
                 "d2h_bytes_per_step": 16 * ne, "ms_per_step": 1e3 * e2e_s},
         "gpu_launches": 3 * args.steps,
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                     "frac": achieved / peak_tflops if peak_tflops else None,
+        "roofline": {"bound": "fp32 (FMA pipe and MUFU)", "achieved": achieved, "peak": peak_tflops,
+                     "unit": "TFLOP/s", "frac": achieved / peak_tflops if peak_tflops else None,
                      "traffic": FAR_TRAFFIC_L6 if args.level == LEVEL else None, "traffic_unit": "bytes per launch",
                      "kernel": "far_kernel<float,7,7,1,true>", "far_ms": far_avg,
                      "flops_per_pair": FLOPS_PER_PAIR,
-                     "peak_source": "FP32 FFMA-chain calibration kernel measured in this run"},
+                     "mufu": {"achieved": mufu, "peak": peak_rsqrt, "unit": "Trsqrt/s",
+                              "frac": mufu / peak_rsqrt if peak_rsqrt else None},
+                     "pair_bound_Gpairs_s": pair_bound / 1e9, "frac_of_pair_bound": pair_rate / pair_bound,
+                     "peak_source": "FFMA-chain and MUFU rsqrt-chain calibration kernels measured in this run "
+                                    "(8 FMA-pipe ops = 16 flops and 1 rsqrt per quadrature pair)"},
         "near_field": {"finalize_ms": fin_avg, "approx_bytes": near_bytes,
                        "GB/s": near_bytes / (fin_avg * 1e-3) / 1e9 if fin_avg > 0 else None},
         "clocks": clocks,
@@ -552,9 +566,10 @@ class _Null:
 def _measure_peak():
     import ctypes
     from easybem_b200 import _lib
-    tf, s = ctypes.c_double(), ctypes.c_double()
+    tf, rs, s = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     _lib.check(_lib.lib().eb_measure_fp32_peak(ctypes.byref(tf), ctypes.byref(s)))
-    return tf.value, s.value
+    _lib.check(_lib.lib().eb_measure_rsqrt_peak(ctypes.byref(rs), ctypes.byref(s)))
+    return tf.value, rs.value
 
 
 if __name__ == "__main__":

@@ -48,6 +48,7 @@ _SIGNATURES = {
     "eb_quadrature": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp,
                                      ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]),
     "eb_measure_fp32_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "eb_measure_rsqrt_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "eb_set_profiling": (ctypes.c_int, [_dp, ctypes.c_int]),
     "eb_dirichlet_rhs": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_evaluate_potential": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]),

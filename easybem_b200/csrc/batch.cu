@@ -93,7 +93,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   EB_CUDA(cudaMemcpy(fin_off_.p, foff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
   EB_CHECK(counter_.alloc(sizeof(int)));
 
-  smem_ = (size_t)src_tile * Q_ * rec_slots(nsl_, false) * (fp32 ? sizeof(float4) : sizeof(dq));
+  smem_ = far_smem_bytes(src_tile, Q_, rec_slots(nsl_, false), fp32);
   int occ = far_occupancy(fp32, nsl_, false, K_, Q_, smem_);
   if (occ < 1) occ = 1;
   int dev = 0, nsm = 148;

@@ -1,8 +1,9 @@
-// Roofline calibration: the sustained FP32 FFMA throughput of this GPU,
-// measured with independent FMA chains (8 per thread, no memory traffic).
-// The far-field kernels are bound by the FP32 pipe, so their roofline
-// fraction is reported against this measured figure rather than a nominal
-// spec-sheet number.
+// Roofline calibration: the sustained FP32 FFMA throughput and the MUFU
+// reciprocal-square-root throughput of this GPU, each measured with
+// independent dependency chains (8 per thread, no memory traffic). The FP32
+// far field needs 8 FMA-pipe operations and 1 MUFU.RSQ per quadrature pair,
+// so both pipes bound it; its roofline fraction is reported against these
+// measured figures rather than nominal spec-sheet numbers.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -26,7 +27,58 @@ __global__ void ffma_chain_kernel(float* out, int iters, float a, float b)
   if (s == 1.2345f) out[blockIdx.x] = s;  // keeps the chains live
 }
 
+__device__ __forceinline__ float rsq_approx(float x)
+{
+  float y;
+  asm volatile("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__global__ void rsqrt_chain_kernel(float* out, int iters)
+{
+  float x[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) x[k] = 1.0f + threadIdx.x + k;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = rsq_approx(x[k]) + 1.0f;
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += x[k];
+  if (s == 1.2345f) out[blockIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace eb
+
+extern "C" int eb_measure_rsqrt_peak(double* tops, double* seconds)
+{
+  if (!tops) return eb::set_error(EB_ERR_INVALID, "null output");
+  int dev = 0, nsm = 0;
+  EB_CUDA(cudaGetDevice(&dev));
+  EB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  float* out = nullptr;
+  EB_CUDA(cudaMalloc(&out, sizeof(float) * 65536));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int threads = 256, blocks = nsm * 8, iters = 2048;
+  eb::rsqrt_chain_kernel<<<blocks, threads>>>(out, 64);  // warm-up
+  cudaEventRecord(e0);
+  eb::rsqrt_chain_kernel<<<blocks, threads>>>(out, iters);
+  cudaEventRecord(e1);
+  cudaError_t err = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (err != cudaSuccess) return eb::set_error(EB_ERR_CUDA, cudaGetErrorString(err));
+  const double ops = 8.0 * iters * (double)threads * blocks;
+  *tops = ops / (ms * 1e-3) / 1e12;
+  if (seconds) *seconds = ms * 1e-3;
+  return EB_OK;
+}
 
 extern "C" int eb_measure_fp32_peak(double* tflops, double* seconds)
 {

@@ -244,14 +244,12 @@ static int build_near(Mesh* m)
   return EB_OK;
 }
 
-static size_t slot_bytes(bool fp32) { return fp32 ? sizeof(float4) : sizeof(dq); }
-
 // Source triangles per shared-memory tile for a variant (whole cells when
 // they fit; large quadrature rules fall back to smaller tiles).
 int src_tile_for(int Q, bool fp32, int nsl, bool dl)
 {
-  const size_t per_tri = (size_t)Q * rec_slots(nsl, dl) * slot_bytes(fp32);
-  const size_t budget = 40 * 1024;
+  const size_t per_tri = far_smem_bytes(1, Q, rec_slots(nsl, dl), fp32);
+  const size_t budget = 48 * 1024;
   int ts = (int)std::min<size_t>(kTS, budget / per_tri);
   return std::max(ts, 1);
 }
@@ -391,7 +389,6 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
   if (!far_variant_supported(nsl, dl)) return set_error(EB_ERR_INVALID, "unsupported operator combination");
   if ((nsl > 0 && (!d_t || !d_v)) || (dl && (!d_u || !d_q))) return set_error(EB_ERR_INVALID, "null vector");
   const int nrec = rec_slots(nsl, dl);
-  const size_t sb = slot_bytes(fp32);
   // Scratch sized once for the largest variant, so device pointers captured
   // in descriptors (and in CUDA graphs) stay valid.
   if (!m->rec.p) {
@@ -401,7 +398,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
   Mesh::Variant& var = m->variants[(fp32 ? 64 : 0) + nsl * 2 + (dl ? 1 : 0)];
   if (!var.desc.p) {
     const FarMeshDesc desc = mesh_far_desc(m, fp32, nsl, dl, m->rec.p, m->partial.as<double>());
-    const size_t smem = (size_t)desc.src_tile * h.Q * nrec * sb;
+    const size_t smem = far_smem_bytes(desc.src_tile, h.Q, nrec, fp32);
     int occ = far_occupancy(fp32, nsl, dl, h.K, h.Q, smem);
     if (occ < 1) occ = 1;
     int nsm = 148;

@@ -9,7 +9,7 @@
 // Launch shape of the far-field kernel: minimum resident CTAs per SM (which
 // caps registers per thread) and the unroll depth of the source-point loop.
 #ifndef EB_F32_MINB
-#define EB_F32_MINB 3
+#define EB_F32_MINB 2
 #endif
 #ifndef EB_F64_MINB
 #define EB_F64_MINB 2
@@ -20,11 +20,15 @@
 #ifndef EB_UNROLL_B_F64
 #define EB_UNROLL_B_F64 1
 #endif
+#ifndef EB_UNROLL_B_X2
+#define EB_UNROLL_B_X2 0  // source-point unroll of the packed FP32 form (0: full)
+#endif
 
 namespace eb {
 
 constexpr int kUnrollF32 = EB_UNROLL_B_F32;
 constexpr int kUnrollF64 = EB_UNROLL_B_F64;
+constexpr int kUnrollX2 = EB_UNROLL_B_X2;
 
 // Neumann/Knuth two-sum accumulation: (s, e) holds s + e exactly up to the
 // rounding of e.
@@ -158,6 +162,136 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
   }
 }
 
+// Packed FP32 form of eval_cell for sm_100 (FFMA2: two FP32 FMAs per issue).
+// Target points are taken in pairs ({x_a, x_a+1}) and every source value is
+// broadcast to both halves ({v, v}), so one pair-instruction evaluates one
+// source point against two target points. Per source point and target pair:
+// 1 FADD2 + 3 FFMA2 for |x - y|^2 (far cells) or 3 FFMA2 + 1 FMUL2 + 2 FFMA2
+// (near cells), 2 MUFU.RSQ, 1 FFMA2 per SL charge and 2 FMUL2 + 1 FFMA2 for
+// the DL sum; an odd last target point runs the scalar form. Each lane of a
+// pair-instruction rounds exactly like the scalar FMA it replaces. The
+// FMA-pipe work per quadrature pair is unchanged (FFMA2 occupies the pipe
+// for two lanes' worth); the pair form halves the issue slots, which bound
+// the scalar loop.
+template <int K, int NQ, int NSL, bool DL, bool FAR>
+__device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, const int4* __restrict__ svid,
+                                             const dq* __restrict__ snrm, const float4* __restrict__ splane, int s0,
+                                             int s1, int nq, int4 tv, const float (&x)[K], const float (&y)[K],
+                                             const float (&z)[K], const float (&q2)[K], const float (&o)[3],
+                                             const double (&cen)[3], const double (&nrm)[3],
+                                             float (&sl)[NSL > 0 ? NSL : 1][K], float (&dl)[K])
+{
+  constexpr int NREC = rec_slots(NSL, DL);
+  constexpr int NS = NSL > 0 ? NSL : 1;
+  constexpr int KP = K / 2;           // packed target pairs
+  constexpr int KP1 = KP > 0 ? KP : 1;
+  constexpr bool ODD = (K & 1) != 0;  // last target point runs scalar
+  constexpr int PS = 4 * NREC;        // staged floats per source point
+  const int nqr = NQ > 0 ? NQ : nq;
+  float2 X[KP1], Y[KP1], Z[KP1], W[KP1], SL[NS][KP1], DLp[KP1];
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+    X[p] = make_float2(x[2 * p], x[2 * p + 1]);
+    Y[p] = make_float2(y[2 * p], y[2 * p + 1]);
+    Z[p] = make_float2(z[2 * p], z[2 * p + 1]);
+    W[p] = make_float2(q2[2 * p], q2[2 * p + 1]);
+    DLp[p] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < NS; ++c) SL[c][p] = make_float2(0.f, 0.f);
+  }
+  const float2 half2 = make_float2(0.5f, 0.5f);
+#pragma unroll 1
+  for (int s = s0; s < s1; ++s) {
+    if constexpr (!FAR) {
+      if (shares_vertex(tv, svid[s])) continue;
+    }
+    const float* r = srec + (size_t)s * nqr * PS;
+    float2 acc2[KP1];
+    float acc1 = 0.f;
+#pragma unroll
+    for (int p = 0; p < KP; ++p) acc2[p] = make_float2(0.f, 0.f);
+#pragma unroll(NQ > 0 ? (kUnrollX2 > 0 ? kUnrollX2 : NQ) : 1)
+    for (int b = 0; b < nqr; ++b) {
+      const float* rb = r + b * PS;
+      const float4* rv = reinterpret_cast<const float4*>(rb);
+      const float4 p0 = rv[0];
+      const float2 px = make_float2(p0.x, p0.x), py = make_float2(p0.y, p0.y);
+      const float2 pz = make_float2(p0.z, p0.z), pw = make_float2(p0.w, p0.w);
+      float2 ch[NS];
+#pragma unroll
+      for (int c = 0; c < NSL; ++c) {
+        const float v = comp(rv[charge_slot(c, DL)], charge_comp(c, DL));
+        ch[c] = make_float2(v, v);
+      }
+      const float2 sdl = DL ? make_float2(rv[1].x, rv[1].x) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int p = 0; p < KP; ++p) {
+        float2 r2;
+        if constexpr (FAR) {
+          r2 = __ffma2_rn(X[p], px, __ffma2_rn(Y[p], py, __ffma2_rn(Z[p], pz, __fadd2_rn(W[p], pw))));
+        } else {
+          const float2 dx = __ffma2_rn(half2, px, X[p]);
+          const float2 dy = __ffma2_rn(half2, py, Y[p]);
+          const float2 dz = __ffma2_rn(half2, pz, Z[p]);
+          r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        }
+        const float2 inv = make_float2(rsq(r2.x), rsq(r2.y));
+#pragma unroll
+        for (int c = 0; c < NSL; ++c) SL[c][p] = __ffma2_rn(ch[c], inv, SL[c][p]);
+        if constexpr (DL) acc2[p] = __ffma2_rn(__fmul2_rn(inv, inv), __fmul2_rn(sdl, inv), acc2[p]);
+      }
+      if constexpr (ODD) {
+        constexpr int a = K - 1;
+        float r2;
+        if constexpr (FAR) {
+          r2 = x[a] * px.x + (y[a] * py.x + (z[a] * pz.x + (q2[a] + pw.x)));
+        } else {
+          const float dx = x[a] + 0.5f * px.x, dy = y[a] + 0.5f * py.x, dz = z[a] + 0.5f * pz.x;
+          r2 = dx * dx + dy * dy + dz * dz;
+        }
+        const float inv = rsq(r2);
+#pragma unroll
+        for (int c = 0; c < NSL; ++c) sl[c][a] += ch[c].x * inv;
+        if constexpr (DL) acc1 += (inv * inv) * (sdl.x * inv);
+      }
+    }
+    if constexpr (DL) {
+      // d = signed distance of each target point from the plane of triangle s
+      float pnx, pny, pnz, pnw;
+      if constexpr (FAR) {
+        const float4 pn = splane[s];
+        pnx = pn.x; pny = pn.y; pnz = pn.z; pnw = -pn.w;
+      } else {
+        const dq nj = snrm[s];
+        pnx = (float)(nj.x - nrm[0]); pny = (float)(nj.y - nrm[1]); pnz = (float)(nj.z - nrm[2]);
+        pnw = (float)(cen[0] * nj.x + cen[1] * nj.y + cen[2] * nj.z - nj.w) + (o[0] * pnx + (o[1] * pny + o[2] * pnz));
+      }
+      const float2 nx = make_float2(pnx, pnx), ny = make_float2(pny, pny), nz = make_float2(pnz, pnz);
+      const float2 nw = make_float2(pnw, pnw);
+#pragma unroll
+      for (int p = 0; p < KP; ++p) {
+        const float2 d = __ffma2_rn(X[p], nx, __ffma2_rn(Y[p], ny, __ffma2_rn(Z[p], nz, nw)));
+        DLp[p] = __ffma2_rn(d, acc2[p], DLp[p]);
+      }
+      if constexpr (ODD) {
+        constexpr int a = K - 1;
+        const float d = x[a] * pnx + (y[a] * pny + (z[a] * pnz + pnw));
+        dl[a] += d * acc1;
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < KP; ++p) {
+#pragma unroll
+    for (int c = 0; c < NS; ++c) {
+      sl[c][2 * p] += SL[c][p].x;
+      sl[c][2 * p + 1] += SL[c][p].y;
+    }
+    dl[2 * p] += DLp[p].x;
+    dl[2 * p + 1] += DLp[p].y;
+  }
+}
+
 // P1T: P1 test functions; the item's three outputs are sum_a w_a phi_k(x_a) acc_a
 // (k = 0, 1, 2 in the triangle's vertex order) of the single SL charge.
 template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
@@ -265,12 +399,22 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
 #pragma unroll
             for (int c = 0; c < NS; ++c) sl[c][a] = 0;
           }
-          if (far)
-            eval_cell<T, K, NQ, NSL, DL, true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
-                                               nrm, sl, dl);
-          else
-            eval_cell<T, K, NQ, NSL, DL, false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
-                                                cen, nrm, sl, dl);
+          if constexpr (F32) {
+            const float* sf = reinterpret_cast<const float*>(s_rec);
+            if (far)
+              eval_cell_x2<K, NQ, NSL, DL, true>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+                                                 nrm, sl, dl);
+            else
+              eval_cell_x2<K, NQ, NSL, DL, false>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+                                                  nrm, sl, dl);
+          } else {
+            if (far)
+              eval_cell<T, K, NQ, NSL, DL, true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
+                                                 cen, nrm, sl, dl);
+            else
+              eval_cell<T, K, NQ, NSL, DL, false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
+                                                  cen, nrm, sl, dl);
+          }
           if constexpr (P1T) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -435,7 +579,9 @@ static cudaError_t launch_far_t(const FarMeshDesc* d_meshes, const WorkItem* d_i
                                 size_t smem, int grid, cudaStream_t st)
 {
   auto kern = far_kernel<T, K, NQ, NSL, DL, P1T>;
-  if (smem > 48 * 1024) {
+  // the kernel's static shared memory (up to ~4 KB) counts against the same
+  // 48 KB default, so opt in above 32 KB of dynamic shared memory
+  if (smem > 32 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
@@ -447,6 +593,8 @@ template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
 static int occupancy_t(size_t smem)
 {
   int nb = 0;
+  if (smem > 32 * 1024)
+    cudaFuncSetAttribute(far_kernel<T, K, NQ, NSL, DL, P1T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_kernel<T, K, NQ, NSL, DL, P1T>, kTT, smem);
   return nb;
 }

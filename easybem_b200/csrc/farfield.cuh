@@ -34,6 +34,12 @@ constexpr int kTT = 128;  // target items (threads) per CTA
 constexpr int kTS = 64;   // source triangles per shared-memory tile (Q <= 7)
 constexpr int kMaxRecSlots = 3;  // record slots of the widest variant
 constexpr int kMaxOutputs = 5;   // SL charges + DL of the widest variant
+// Shared memory of a staged source tile: 16 bytes per FP32 record slot,
+// 32 per FP64 slot.
+__host__ __device__ constexpr size_t far_smem_bytes(int src_tile, int Q, int nrec, bool fp32)
+{
+  return (size_t)src_tile * Q * nrec * (fp32 ? 16 : 32);
+}
 constexpr int kPrepBlock = 256;     // threads per block of the record preparation (one source point each)
 constexpr int kFinalizeBlock = 128; // threads per block of the finalize (one output row each)
 

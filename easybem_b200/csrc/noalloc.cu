@@ -95,7 +95,7 @@ extern "C" int eb_apply_sl_dl_noalloc(eb_mesh handle, int precision, const doubl
   cudaStream_t st = (cudaStream_t)stream;
 
   const FarMeshDesc desc = mesh_far_desc(m, fp32, nsl, dl, rec, partial);
-  const size_t smem = (size_t)desc.src_tile * h.Q * nrec * slot;
+  const size_t smem = far_smem_bytes(desc.src_tile, h.Q, nrec, fp32);
   int occ = far_occupancy(fp32, nsl, dl, h.K, h.Q, smem);
   if (occ < 1) occ = 1;
   int nsm = 148;

@@ -162,11 +162,10 @@ int mesh_apply_sl_p1(Mesh* m, int precision, const double* d_t, double* d_v, cud
     EB_CHECK(m->rec.alloc((size_t)h.ne * h.Q * kMaxRecSlots * sizeof(dq)));
     EB_CHECK(m->partial.alloc(sizeof(double) * (size_t)kMaxOutputs * m->plan.nsplit * h.nitems));
   }
-  const size_t sb = fp32 ? sizeof(float4) : sizeof(dq);
   Mesh::Variant& var = m->variants[100 + (fp32 ? 1 : 0)];
   if (!var.desc.p) {
     const FarMeshDesc desc = mesh_far_desc(m, fp32, 1, false, m->rec.p, m->partial.as<double>());
-    const size_t smem = (size_t)desc.src_tile * h.Q * rec_slots(1, false) * sb;
+    const size_t smem = far_smem_bytes(desc.src_tile, h.Q, rec_slots(1, false), fp32);
     int occ = far_occupancy(fp32, 1, false, h.K, h.Q, smem, true);
     if (occ < 1) occ = 1;
     int nsm = 148;

@@ -135,7 +135,13 @@ class Server {
     cudaSetDevice(device_);
     // join prepared requests (slots permitting)
     {
-      std::lock_guard<std::mutex> g(mu_);
+      std::unique_lock<std::mutex> g(mu_);
+      // nothing to run yet but meshes in preparation: wait (bounded) for the
+      // first one instead of returning at once, so callers need not spin
+      if (active_.empty() && prepared_.empty() && (preparing_ > 0 || !to_prepare_.empty()))
+        ready_cv_.wait_for(g, std::chrono::milliseconds(100), [this] {
+          return stop_ || !prepared_.empty() || (preparing_ == 0 && to_prepare_.empty());
+        });
       for (auto it = prepared_.begin(); it != prepared_.end();) {
         auto r = *it;
         if (active_systems_ + r->nrhs > max_systems_ && active_systems_ > 0) break;
@@ -282,6 +288,7 @@ class Server {
       std::string err = rc == EB_OK ? "" : last_error();
       std::lock_guard<std::mutex> g(mu_);
       preparing_--;
+      ready_cv_.notify_all();  // under the lock: step() sees the new state once it wakes
       if (rc != EB_OK) {
         if (m) eb_mesh_destroy(m);
         r->state = 5;
@@ -310,6 +317,7 @@ class Server {
   int device_ = 0;
   std::mutex mu_;
   std::condition_variable cv_;
+  std::condition_variable ready_cv_;  // a prepared (or failed) request is ready for step()
   bool stop_ = false;
   std::thread worker_;
   long long next_id_ = 1;

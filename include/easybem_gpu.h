@@ -207,6 +207,10 @@ int eb_quadrature(int order, int* nline, double* lx, double* lw, int* ntri, doub
  * TFLOP/s (FMA = 2 flops), from a register-only FMA-chain kernel. No
  * counterpart in the reference. */
 int eb_measure_fp32_peak(double* tflops, double* seconds);
+/* MUFU reciprocal-square-root throughput of the current GPU in Tops/s (one
+ * rsqrt.approx.f32 per far-field quadrature pair), from a chain kernel. No
+ * counterpart in the reference. */
+int eb_measure_rsqrt_peak(double* tops, double* seconds);
 
 /* Event timing of the far-field kernel and of the finalize kernel (which
  * includes the near-field SpMV) of the last apply on this mesh, recorded on
