@@ -155,6 +155,13 @@ class Mesh:
         check(lib().eb_dirichlet_rhs(self._h, g2.shape[0], _ptr(g2), _ptr(b)))
         return b[0] if one else b
 
+    def apply_near_precond(self, x):
+        """y = M x with the solver's preconditioner (sparse approximate inverse of the near field)."""
+        x = _vec(x, self.nelems, "x")
+        y = np.empty(self.nelems)
+        check(lib().eb_apply_near_precond(self._h, _ptr(x), _ptr(y)))
+        return y
+
     def set_profiling(self, on: bool = True):
         check(lib().eb_set_profiling(self._h, 1 if on else 0))
 
@@ -244,8 +251,9 @@ class Solver:
     """
 
     def __init__(self, tol=1e-8, inner_tol=1e-6, restart=50, max_cycles=40, max_iterations=4000,
-                 inner_precision="mixed"):
-        o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision))
+                 inner_precision="mixed", precond=True):
+        o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision),
+                         1 if precond else 0)
         h = ctypes.c_void_p()
         check(lib().eb_solver_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h
@@ -309,8 +317,9 @@ class Server:
     STATES = {0: "queued", 1: "preparing", 2: "prepared", 3: "solving", 4: "done", 5: "failed"}
 
     def __init__(self, budget_bytes: int, max_systems: int = 4096, tol=1e-8, inner_tol=1e-6, restart=50,
-                 max_cycles=40, max_iterations=4000, inner_precision="mixed"):
-        o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision))
+                 max_cycles=40, max_iterations=4000, inner_precision="mixed", precond=True):
+        o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision),
+                         1 if precond else 0)
         h = ctypes.c_void_p()
         check(lib().eb_server_create(int(budget_bytes), int(max_systems), ctypes.byref(o), ctypes.byref(h)))
         self._h = h

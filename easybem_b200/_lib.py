@@ -53,6 +53,7 @@ _SIGNATURES = {
     "eb_dirichlet_rhs": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_evaluate_potential": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]),
     "eb_solve_options_default": (None, [_dp]),
+    "eb_apply_near_precond": (ctypes.c_int, [_dp, _dp, _dp]),
     "eb_solve_sl": (ctypes.c_int, [ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]),
     "eb_solver_create": (ctypes.c_int, [_dp, ctypes.POINTER(_dp)]),
     "eb_solver_destroy": (ctypes.c_int, [_dp]),
@@ -90,7 +91,8 @@ _SIGNATURES = {
 
 class SolveOptions(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("inner_tol", ctypes.c_double), ("restart", ctypes.c_int),
-                ("max_cycles", ctypes.c_int), ("max_iterations", ctypes.c_int), ("inner_precision", ctypes.c_int)]
+                ("max_cycles", ctypes.c_int), ("max_iterations", ctypes.c_int), ("inner_precision", ctypes.c_int),
+                ("precond", ctypes.c_int)]
 
 
 class SolveStats(ctypes.Structure):

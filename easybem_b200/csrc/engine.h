@@ -59,6 +59,8 @@ struct Mesh {
   DevBuf p1_rowptr, p1_col, p1_val;
   // near field
   DevBuf sl_rowptr, sl_col, sl_val, dl_rowptr, dl_col, dl_val;
+  // near-field sparse approximate inverse of V (solver preconditioner, built on first use)
+  DevBuf pc_val;
   long long npairs = 0;
   // per-apply scratch
   DevBuf rec, partial, counter, items;
@@ -109,6 +111,10 @@ int mesh_apply_sl_p1(Mesh* m, int precision, const double* d_t, double* d_v, cud
 int mesh_set_plan(Mesh* m, int items_per_sm, int tile);
 // The tuned plan recorded for meshes like m (returns false if none).
 bool tuned_plan_for(const HostMesh& h, int* items_per_sm, int* tile);
+// Sparse approximate inverse of the SL near field on its own pattern (built once).
+int ensure_near_precond(Mesh* m);
+// y = M x with that inverse (original triangle order, device vectors).
+cudaError_t near_precond_apply(const Mesh* m, const double* d_x, double* d_y, cudaStream_t st);
 // vertex -> (triangle, local index) lists on the device (built on first use)
 int ensure_vertex_lists(Mesh* m);
 // q = D u (hypersingular, curl form); u and q have nnodes entries (device).

@@ -49,7 +49,7 @@ static size_t mesh_resident_bytes(const Mesh* m)
                           &m->tgt32, &m->tgt64, &m->tcent, &m->tnrm, &m->tvid, &m->ccent, &m->snrm, &m->ttile,
                           &m->splane32, &m->splane64, &m->sl_rowptr, &m->sl_col, &m->sl_val, &m->dl_rowptr,
                           &m->dl_col, &m->dl_val, &m->rec, &m->partial, &m->counter, &m->items, &m->io_t,
-                          &m->io_u, &m->io_v, &m->io_q};
+                          &m->io_u, &m->io_v, &m->io_q, &m->pc_val};
   for (const DevBuf* d : bufs) b += d->bytes;
   return b;
 }
@@ -61,7 +61,7 @@ static size_t estimate_bytes(int nv, int ne, int order, int nrhs, int restart)
   Quadrature q;
   make_quadrature(order, &q);
   const size_t Q = q.nt;
-  const size_t mesh = (size_t)ne * (13 * (12 + 40) + 400 + Q * (16 + 32 + 8 + 16 + 32 + 3 * 32)) + (size_t)nv * 40;
+  const size_t mesh = (size_t)ne * (13 * (12 + 48) + 400 + Q * (16 + 32 + 8 + 16 + 32 + 3 * 32)) + (size_t)nv * 40;
   const size_t solver = (size_t)nrhs * ne * 8 * (restart + 4) + ((size_t)nrhs + 3) / 4 * ne * (Q * 64 + 160);
   return mesh + solver;
 }
@@ -285,6 +285,7 @@ class Server {
         b.resize((size_t)r->nrhs * r->ne);
         rc = eb_dirichlet_rhs(m, r->nrhs, r->g.data(), b.data());
       }
+      if (rc == EB_OK && opt_.precond) rc = ensure_near_precond(eb_mesh_internal(m));
       std::string err = rc == EB_OK ? "" : last_error();
       std::lock_guard<std::mutex> g(mu_);
       preparing_--;
@@ -348,7 +349,9 @@ int eb_server_create(long long budget_bytes, int max_systems, const eb_solve_opt
     o.max_cycles = opt->max_cycles;
     o.max_iterations = opt->max_iterations;
     o.inner_precision = opt->inner_precision;
+    o.precond = opt->precond;
   }
+  if (o.precond != 0 && o.precond != 1) return set_error(EB_ERR_INVALID, "precond must be 0 or 1");
   auto s = new eb_server_s();
   s->srv = std::make_unique<eb::Server>((size_t)budget_bytes, max_systems, o);
   *out = s;

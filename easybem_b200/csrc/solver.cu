@@ -30,15 +30,29 @@ __device__ double block_sum(double v)
 struct SysDevK {
   int ne;
   double *basis, *x, *b, *r, *tin, *vout;
+  const int *prow, *pcol;
+  const double* pval;
 };
 
+// y_i = (M v)_i for one row with the near-field-pattern preconditioner
+__device__ __forceinline__ double precond_row(const SysDevK& t, const double* v, int i)
+{
+  double acc = 0.0;
+  for (int p = t.prow[i]; p < t.prow[i + 1]; ++p) acc += t.pval[p] * v[t.pcol[p]];
+  return acc;
+}
+
+// apply input: the refinement residual uses x; an Arnoldi step uses M v_k
+// (right preconditioning: GMRES runs on V M, and x = M y)
 __global__ void k_load(const SysDevK* T, const int* phase, const int* kk, int want, int from_basis)
 {
   const int s = blockIdx.y;
   if (phase[s] != want) return;
   const SysDevK t = T[s];
   const double* src = from_basis ? t.basis + (size_t)kk[s] * t.ne : t.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.ne; i += gridDim.x * blockDim.x) t.tin[i] = src[i];
+  const bool pc = from_basis && t.pval;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.ne; i += gridDim.x * blockDim.x)
+    t.tin[i] = pc ? precond_row(t, src, i) : src[i];
 }
 
 __global__ void k_residual(const SysDevK* T, const int* phase, const int* fresh, int want)
@@ -112,6 +126,8 @@ __global__ void k_start(const SysDevK* T, const int* flag, const double* rn)
     t.basis[i] = t.r[i] * inv;
 }
 
+// x += sum_j y_j v_j, or with the preconditioner z = sum_j y_j v_j (into r,
+// free until the next refinement residual) and then x += M z (k_xprecond)
 __global__ void k_xupdate(const SysDevK* T, const int* flag, int m, const double* y)
 {
   const int s = blockIdx.y;
@@ -122,8 +138,19 @@ __global__ void k_xupdate(const SysDevK* T, const int* flag, int m, const double
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.ne; i += gridDim.x * blockDim.x) {
     double acc = 0.0;
     for (int j = 0; j < nk; j++) acc += ys[j] * t.basis[(size_t)j * t.ne + i];
-    t.x[i] += acc;
+    if (t.pval) t.r[i] = acc;
+    else t.x[i] += acc;
   }
+}
+
+__global__ void k_xprecond(const SysDevK* T, const int* flag)
+{
+  const int s = blockIdx.y;
+  if (flag[s] <= 0) return;
+  const SysDevK t = T[s];
+  if (!t.pval) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.ne; i += gridDim.x * blockDim.x)
+    t.x[i] += precond_row(t, t.r, i);
 }
 
 }  // namespace
@@ -141,6 +168,7 @@ int SolverPool::add(Mesh* m, int nrhs, const double* b_host, int* ids)
   for (const auto& s : sys_)
     if (s->entry->mesh->h.Q != m->h.Q)
       return set_error(EB_ERR_INVALID, "all meshes of a solve need the same quadrature order");
+  if (opt_.precond) EB_CHECK(ensure_near_precond(m));
   const int ne = m->h.ne;
   for (int c0 = 0; c0 < nrhs; c0 += kBatchCols) {
     auto e = std::make_unique<BatchEntry>();
@@ -194,8 +222,12 @@ int SolverPool::rebuild()
   std::vector<SysDev> tab(S);
   for (int s = 0; s < S; s++) {
     Sys& y = *sys_[s];
+    const Mesh* mm = y.entry->mesh;
+    const bool pc = opt_.precond && mm->pc_val.p;
     tab[s] = SysDev{y.ne, y.basis.as<double>(), y.x.as<double>(), y.b.as<double>(), y.r.as<double>(),
-                    y.entry->tin.as<double>() + (size_t)y.col * y.ne, y.entry->vout.as<double>() + (size_t)y.col * y.ne};
+                    y.entry->tin.as<double>() + (size_t)y.col * y.ne, y.entry->vout.as<double>() + (size_t)y.col * y.ne,
+                    pc ? mm->sl_rowptr.as<int>() : nullptr, pc ? mm->sl_col.as<int>() : nullptr,
+                    pc ? mm->pc_val.as<double>() : nullptr};
   }
   const size_t n1 = std::max(S, 1);
   EB_CHECK(d_tab_.alloc(sizeof(SysDev) * n1));
@@ -345,7 +377,10 @@ int SolverPool::step(cudaStream_t st, int* nactive)
       for (int j = 0; j <= k; j++) q.H[(size_t)j * m + k] = h[j];
       q.k = k + 1;
       q.iterations++;
-      const bool inner_done = std::fabs(q.g[q.k]) <= opt_.inner_tol * q.beta || q.k == m || !(wn_[s] > 0) ||
+      // a cycle stops at the inner reduction, or as soon as its estimate
+      // already meets the outer target (the next FP64 residual decides)
+      const double stop = std::max(opt_.inner_tol * q.beta, 0.5 * opt_.tol * q.bnorm);
+      const bool inner_done = std::fabs(q.g[q.k]) <= stop || q.k == m || !(wn_[s] > 0) ||
                               q.iterations >= opt_.max_iterations;
       if (inner_done) {
         // back substitution H(0:k,0:k) y = g(0:k)
@@ -366,6 +401,7 @@ int SolverPool::step(cudaStream_t st, int* nactive)
     EB_CUDA(cudaMemcpyAsync(d_y_.p, y.data(), sizeof(double) * S * m, cudaMemcpyHostToDevice, st));
     EB_CUDA(cudaMemcpyAsync(d_flag_x_.p, fx_.data(), sizeof(int) * S, cudaMemcpyHostToDevice, st));
     k_xupdate<<<eg, 256, 0, st>>>(T, d_flag_x_.as<int>(), m, d_y_.as<double>());
+    if (opt_.precond) k_xprecond<<<eg, 256, 0, st>>>(T, d_flag_x_.as<int>());
   }
   if (any_start) {
     EB_CUDA(cudaMemcpyAsync(d_flag_start_.p, fstart_.data(), sizeof(int) * S, cudaMemcpyHostToDevice, st));
@@ -438,6 +474,7 @@ static eb::SolveOptions to_options(const eb_solve_options* o)
     r.max_cycles = o->max_cycles;
     r.max_iterations = o->max_iterations;
     r.inner_precision = o->inner_precision;
+    r.precond = o->precond;
   }
   return r;
 }
@@ -454,6 +491,7 @@ void eb_solve_options_default(eb_solve_options* o)
   o->max_cycles = d.max_cycles;
   o->max_iterations = d.max_iterations;
   o->inner_precision = d.inner_precision;
+  o->precond = d.precond;
 }
 
 int eb_solver_create(const eb_solve_options* opt, eb_solver* out)
@@ -464,6 +502,7 @@ int eb_solver_create(const eb_solve_options* opt, eb_solver* out)
     return set_error(EB_ERR_INVALID, "invalid solve options");
   if (o.inner_precision != EB_PREC_FP64 && o.inner_precision != EB_PREC_MIXED)
     return set_error(EB_ERR_INVALID, "inner precision must be EB_PREC_FP64 or EB_PREC_MIXED");
+  if (o.precond != 0 && o.precond != 1) return set_error(EB_ERR_INVALID, "precond must be 0 or 1");
   auto s = new eb_solver_s();
   s->pool = std::make_unique<eb::SolverPool>(o);
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);

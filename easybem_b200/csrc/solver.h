@@ -32,6 +32,7 @@ struct SolveOptions {
   int max_cycles = 40;      // refinement cycles per system
   int max_iterations = 4000;
   int inner_precision = EB_PREC_MIXED;
+  int precond = 1;          // 1: near-field sparse approximate inverse (right), 0: none
 };
 
 struct SolveStats {
@@ -73,6 +74,8 @@ class SolverPool {
   struct SysDev {
     int ne;
     double *basis, *x, *b, *r, *tin, *vout;
+    const int *prow, *pcol;  // right preconditioner M on the near-field pattern (null: none)
+    const double* pval;
   };
   int rebuild();
   int upload_control(cudaStream_t st);

@@ -132,6 +132,12 @@ typedef struct eb_solve_options {
   int max_cycles;      /* refinement cycles per system (default 40) */
   int max_iterations;  /* GMRES iterations per system (default 4000) */
   int inner_precision; /* EB_PREC_MIXED (default) or EB_PREC_FP64 */
+  int precond;         /* 1 (default): right preconditioner M, the sparse
+                        * approximate inverse of the FP64 near field on its own
+                        * pattern (column j minimises ||N m - e_j|| over the
+                        * triangles sharing a vertex with j); 0: none. It changes
+                        * the iteration count only: every cycle ends with the
+                        * true FP64 residual of V x = b. */
 } eb_solve_options;
 
 typedef struct eb_solve_stats {
@@ -142,6 +148,9 @@ typedef struct eb_solve_stats {
 } eb_solve_stats;
 
 void eb_solve_options_default(eb_solve_options* opt);
+/* y = M x with the solver's near-field preconditioner (built on first use);
+ * x and y have nelems entries, host memory. No counterpart in the reference. */
+int eb_apply_near_precond(eb_mesh mesh, const double* x, double* y);
 /* Solves sum(nrhs) systems at once: b[i] and x[i] are host arrays
  * [nrhs[i]][nelems of meshes[i]]; stats (optional) has one entry per system
  * in mesh-major order. All meshes need the same quadrature order. Returns

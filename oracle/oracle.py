@@ -168,6 +168,36 @@ class Oracle:
         return vij.value, k, col
 
 
+def near_spai(V, elems):
+    """Sparse approximate inverse of the near field of V (dense FP64 [ne, ne],
+    row = test triangle), as the solver's preconditioner defines it
+    (easybem_b200/csrc/precond.cu): N keeps the entries of the triangle pairs
+    that share a vertex; column j of M minimises ||N m - e_j||_2 over vectors
+    supported on the triangles sharing a vertex with j. Solved here with a
+    least-squares routine (the GPU forms the normal equations); returns M
+    dense. Not from the reference, which has no preconditioner."""
+    V = np.asarray(V, dtype=np.float64)
+    f = np.asarray(elems) - 1
+    ne = f.shape[0]
+    by_vertex = {}
+    for i, tri in enumerate(f):
+        for v in tri:
+            by_vertex.setdefault(int(v), []).append(i)
+    ring = [sorted(set(k for v in f[i] for k in by_vertex[int(v)])) for i in range(ne)]
+    N = np.zeros_like(V)
+    for i in range(ne):
+        N[i, ring[i]] = V[i, ring[i]]
+    M = np.zeros_like(V)
+    for j in range(ne):
+        J = ring[j]
+        I = sorted(set(i for k in J for i in ring[k]))
+        e = np.zeros(len(I))
+        e[I.index(j)] = 1.0
+        m, *_ = np.linalg.lstsq(N[np.ix_(I, J)], e, rcond=None)
+        M[J, j] = m
+    return M
+
+
 def ref_set_order(order: int):
     ref_lib().ref_set_order(order)
 

@@ -37,9 +37,10 @@ def test_dirichlet_solve_sphere_matches_dense_reference(gpu_lib, oracle):
         b = m.dirichlet_rhs(g)
         assert rel_l2(b, b_ref) < 1e-12
         for prec in ("mixed", "fp64"):
-            [(t, stats)] = gpu_lib.solve([(m, b)], tol=1e-8, inner_precision=prec)
-            assert stats[0]["converged"] and stats[0]["rel_residual"] <= 1e-8
-            assert rel_l2(t, t_ref) < 1e-6
+            for pc in (True, False):
+                [(t, stats)] = gpu_lib.solve([(m, b)], tol=1e-8, inner_precision=prec, precond=pc)
+                assert stats[0]["converged"] and stats[0]["rel_residual"] <= 1e-8
+                assert rel_l2(t, t_ref) < 1e-6
     # discretisation error against the exact Neumann data du/dn at centroids
     P = nodes[elems - 1]
     c = P.mean(axis=1)
@@ -104,3 +105,40 @@ def test_stepwise_solver_admits_systems_between_steps(gpu_lib):
     s.close()
     for m in ms:
         m.close()
+
+
+def test_near_field_preconditioner_cuts_iterations_not_accuracy(gpu_lib):
+    # torus of the serving workload and a stretched ellipsoid: the same
+    # solution (both reach the FP64 residual target) in far fewer iterations
+    cases = [meshes.torus(64, 0.3)]
+    v, f = meshes.icosphere(4)
+    cases.append((v * np.array([2.0, 1.0, 0.5]), f))
+    for nodes, elems in cases:
+        x0 = np.array([0.3, -0.2, 4.0])
+        g = 1.0 / np.linalg.norm(nodes - x0, axis=1)
+        with gpu_lib.Mesh(nodes, elems) as m:
+            b = m.dirichlet_rhs(g)
+            [(t0, s0)] = gpu_lib.solve([(m, b)], tol=1e-8, precond=False)
+            [(t1, s1)] = gpu_lib.solve([(m, b)], tol=1e-8, precond=True)
+            assert s0[0]["converged"] and s1[0]["converged"]
+            assert s1[0]["rel_residual"] <= 1e-8
+            assert rel_l2(t1, t0) < 1e-6
+            assert 3 * s1[0]["iterations"] <= s0[0]["iterations"], (s0[0]["iterations"], s1[0]["iterations"])
+
+
+def test_preconditioner_matches_oracle_restatement(gpu_lib, oracle):
+    # the GPU normal-equation build against a least-squares restatement on the
+    # pinned FP64 near-field values, and its effect: V M close to identity
+    from oracle.oracle import near_spai
+    nodes, elems = meshes.perturbed_icosphere(2, seed=8)
+    oracle.set_order(4)
+    V, _ = oracle.dense(nodes, elems)
+    M = near_spai(V, elems)
+    rng = np.random.default_rng(4)
+    with gpu_lib.Mesh(nodes, elems) as m:
+        for _ in range(3):
+            x = rng.normal(size=elems.shape[0])
+            assert rel_l2(m.apply_near_precond(x), M @ x) < 1e-9
+    VM = np.asarray(V) @ M
+    ev = np.linalg.svd(VM, compute_uv=False)
+    assert ev[0] / ev[-1] < np.linalg.cond(np.asarray(V)) / 3
