@@ -107,6 +107,74 @@ __global__ void __launch_bounds__(kPotThreads) potential_kernel(int npts, const 
   if (active) partial[(size_t)blockIdx.y * npts + i] = (double)hi + (double)lo;
 }
 
+// FP32 form for sm_100: each thread owns two evaluation points (i and
+// i + kPotThreads of the block's 2 * kPotThreads) and evaluates them together
+// with packed FFMA2/FMUL2, every source value broadcast to both halves; the
+// arithmetic per lane is that of the scalar kernel above.
+__global__ void __launch_bounds__(kPotThreads) potential_x2_kernel(int npts, const double* __restrict__ pts, int ne,
+                                                                   int Q, int cells_per_chunk,
+                                                                   const float4* __restrict__ rec,
+                                                                   const float4* __restrict__ plane,
+                                                                   const dq* __restrict__ ccent,
+                                                                   double* __restrict__ partial)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* s_rec = reinterpret_cast<float4*>(smem_raw);
+  __shared__ float4 s_plane[kTS];
+  const int i0 = blockIdx.x * 2 * kPotThreads + threadIdx.x, i1 = i0 + kPotThreads;
+  const bool a0 = i0 < npts, a1 = i1 < npts;
+  double px[2], py[2], pz[2];
+  px[0] = a0 ? pts[3 * i0] : 0.0; py[0] = a0 ? pts[3 * i0 + 1] : 0.0; pz[0] = a0 ? pts[3 * i0 + 2] : 0.0;
+  px[1] = a1 ? pts[3 * i1] : px[0]; py[1] = a1 ? pts[3 * i1 + 1] : py[0]; pz[1] = a1 ? pts[3 * i1 + 2] : pz[0];
+  const int ncells = (ne + kCell - 1) / kCell;
+  const int c0 = blockIdx.y * cells_per_chunk, c1 = min(ncells, c0 + cells_per_chunk);
+  const int sb = c0 * kCell, se = min(ne, c1 * kCell);
+  const float2 half2 = make_float2(0.5f, 0.5f);
+  float hi[2] = {0.f, 0.f}, lo[2] = {0.f, 0.f};
+  for (int t0 = sb; t0 < se; t0 += kTS) {
+    const int ns = min(kTS, se - t0);
+    for (int k = threadIdx.x; k < ns * Q * 2; k += kPotThreads) s_rec[k] = rec[(size_t)t0 * Q * 2 + k];
+    for (int k = threadIdx.x; k < ns; k += kPotThreads) s_plane[k] = plane[t0 + k];
+    __syncthreads();
+    if (a0) {
+      for (int g0 = 0; g0 < ns;) {
+        const int cell = (t0 + g0) / kCell;
+        const int g1 = min(ns, (cell + 1) * kCell - t0);
+        const dq cc = ccent[cell];
+        const float2 X = make_float2((float)(px[0] - cc.x), (float)(px[1] - cc.x));
+        const float2 Y = make_float2((float)(py[0] - cc.y), (float)(py[1] - cc.y));
+        const float2 Z = make_float2((float)(pz[0] - cc.z), (float)(pz[1] - cc.z));
+        float2 part = make_float2(0.f, 0.f);
+        for (int s = g0; s < g1; ++s) {
+          const float4 pn = s_plane[s];
+          const float2 d = __ffma2_rn(X, make_float2(pn.x, pn.x),
+                                      __ffma2_rn(Y, make_float2(pn.y, pn.y),
+                                                 __ffma2_rn(Z, make_float2(pn.z, pn.z), make_float2(-pn.w, -pn.w))));
+          float2 sl = make_float2(0.f, 0.f), acc = make_float2(0.f, 0.f);
+          const float4* r = s_rec + (size_t)s * Q * 2;
+          for (int b = 0; b < Q; ++b) {
+            const float4 p0 = r[2 * b], p1 = r[2 * b + 1];
+            const float2 dx = __ffma2_rn(half2, make_float2(p0.x, p0.x), X);
+            const float2 dy = __ffma2_rn(half2, make_float2(p0.y, p0.y), Y);
+            const float2 dz = __ffma2_rn(half2, make_float2(p0.z, p0.z), Z);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            const float2 inv = make_float2(pot_rsq(r2.x), pot_rsq(r2.y));
+            sl = __ffma2_rn(make_float2(p1.y, p1.y), inv, sl);
+            acc = __ffma2_rn(__fmul2_rn(inv, inv), __fmul2_rn(make_float2(p1.x, p1.x), inv), acc);
+          }
+          part = __fadd2_rn(part, __ffma2_rn(make_float2(-d.x, -d.y), acc, sl));
+        }
+        pot_two_sum(hi[0], lo[0], part.x);
+        pot_two_sum(hi[1], lo[1], part.y);
+        g0 = g1;
+      }
+    }
+    __syncthreads();
+  }
+  if (a0) partial[(size_t)blockIdx.y * npts + i0] = (double)hi[0] + (double)lo[0];
+  if (a1) partial[(size_t)blockIdx.y * npts + i1] = (double)hi[1] + (double)lo[1];
+}
+
 __global__ void potential_reduce_kernel(int npts, int nchunk, const double* __restrict__ partial,
                                         double* __restrict__ out)
 {
@@ -135,7 +203,8 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
   EB_CUDA(prep_launch(fp32, 1, true, A, st));
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-  const int pblocks = (npts + kPotThreads - 1) / kPotThreads;
+  const int per_block = fp32 ? 2 * kPotThreads : kPotThreads;  // the FP32 kernel takes two points per thread
+  const int pblocks = (npts + per_block - 1) / per_block;
   int nchunk = std::max(1, std::min(h.ncells, (4 * nsm + pblocks - 1) / pblocks));
   const int cells_per = (h.ncells + nchunk - 1) / nchunk;
   nchunk = (h.ncells + cells_per - 1) / cells_per;
@@ -143,13 +212,13 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
   const size_t smem = (size_t)kTS * h.Q * 2 * (fp32 ? sizeof(float4) : sizeof(dq));
   const dim3 grid(pblocks, nchunk);
   if (fp32) {
-    auto k = potential_kernel<float>;
-    if (smem > 48 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto k = potential_x2_kernel;
+    if (smem > 32 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, m->rec.as<float4>(),
                                        m->splane32.as<float4>(), m->ccent.as<dq>(), m->pot_partial.as<double>());
   } else {
     auto k = potential_kernel<double>;
-    if (smem > 48 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem > 32 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, m->rec.as<dq>(), m->splane64.as<dq>(),
                                        m->ccent.as<dq>(), m->pot_partial.as<double>());
   }
