@@ -506,7 +506,9 @@ def main():
     mufu = pair_rate * RSQRT_PER_PAIR / 1e12
     # the pair rate both pipes allow together, and the fraction of it reached
     pair_bound = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
-    near_bytes = 12 * mesh.near_pairs + 8 * ne * 13 * 3  # SL CSR + DL CSR values/cols (approx.)
+    nb = ctypes.c_longlong()
+    _lib.check(L.eb_mesh_finalize_bytes(mesh.handle, ctypes.byref(nb)))
+    near_bytes = nb.value  # near-field CSR + gathered densities + far partial sums + outputs
     cpu = None if args.no_cpu_baseline else cpu_reference_sample(nodes, elems, t, u)
     clocks = sampler.summary()
     serve = None
@@ -538,8 +540,10 @@ def main():
                      "pair_bound_Gpairs_s": pair_bound / 1e9, "frac_of_pair_bound": pair_rate / pair_bound,
                      "peak_source": "FFMA-chain and MUFU rsqrt-chain calibration kernels measured in this run "
                                     "(8 FMA-pipe ops = 16 flops and 1 rsqrt per quadrature pair)"},
-        "near_field": {"finalize_ms": fin_avg, "approx_bytes": near_bytes,
-                       "GB/s": near_bytes / (fin_avg * 1e-3) / 1e9 if fin_avg > 0 else None},
+        "near_field": {"kernel": "finalize_kernel<1,1> (near-field SpMV + partial-sum fold)",
+                       "finalize_ms": fin_avg, "algorithmic_bytes": near_bytes,
+                       "GB/s": near_bytes / (fin_avg * 1e-3) / 1e9 if fin_avg > 0 else None,
+                       "hbm_peak_GB/s": _hbm_peak(), "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
         "clocks": clocks,
     }
     if cpu is not None:
@@ -561,6 +565,14 @@ class _Null:
 
     def __exit__(self, *exc):
         return False
+
+
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh).get("hbm_gbs")
+    except (OSError, ValueError):
+        return None
 
 
 def _measure_peak():

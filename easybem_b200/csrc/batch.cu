@@ -60,7 +60,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
                               be->vout.as<double>(), h.ne, nullptr);
     args[e].active = d_flags ? d_flags + e : nullptr;
     poff[e + 1] = poff[e] + (int)(((long long)h.ne * h.Q + kPrepBlock - 1) / kPrepBlock);
-    foff[e + 1] = foff[e] + (h.ne + kFinalizeBlock - 1) / kFinalizeBlock;
+    foff[e + 1] = foff[e] + (h.ne + kFinalizeRows - 1) / kFinalizeRows;
     quad_pairs_ += h.far_quad_pairs;
     for (WorkItem w : m->items_host) {
       w.mesh = e;

@@ -493,6 +493,19 @@ int eb_mesh_info(eb_mesh mesh, int* nnodes, int* nelems, long long* near_pairs, 
   return EB_OK;
 }
 
+int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes)
+{
+  if (!mesh || !bytes) return set_error(EB_ERR_INVALID, "null argument");
+  const eb::HostMesh& h = mesh->m->h;
+  const long long ne = h.ne, sl = (long long)h.sl_col.size(), dl = (long long)h.dl_col.size();
+  // per row: CSR row pointers, per entry column + value + gathered density,
+  // the far-field partial sums of both outputs, the two outputs
+  long long b = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8);
+  b += 2 * 8LL * mesh->m->plan.nsplit * h.nitems + 2 * 8 * ne + 8 * ne /* trin */ + 4 * ne /* iperm */;
+  *bytes = b;
+  return EB_OK;
+}
+
 int eb_apply_sl_dl_device(eb_mesh mesh, int precision, const double* d_t, const double* d_u, double* d_v,
                           double* d_q, void* stream)
 {

@@ -498,32 +498,57 @@ __device__ __forceinline__ void prep_point(const ApplyArgs& A, long long idx)
   }
 }
 
-// Output row i (original order): sum the partial slots of the triangle's
-// items in a fixed order, scale by J_i / (4 pi) and add the FP64 near field.
-template <int NSL, bool DL>
-__device__ __forceinline__ void finalize_row(const ApplyArgs& A, int i)
+// Output rows in sorted (Morton) order, kFinalizeLanes threads per row: the
+// lanes take every kFinalizeLanes-th partial slot and CSR entry, then add
+// their sums in a fixed shuffle tree (deterministic). Sorted order makes the
+// partial-sum reads of neighbouring rows contiguous; the row's original index
+// i = perm[s] addresses the near-field CSR and the outputs. Result: far sum
+// times J_i / (4 pi) plus the FP64 near field.
+__device__ __forceinline__ double lanes_sum(double v)
 {
-  if (i >= A.ne || (A.active && *A.active == 0)) return;
-  const int s = A.iperm[i];
-  const double scale = A.trin[s].w * (0.25 / M_PI);
+#pragma unroll
+  for (int o = 1; o < kFinalizeLanes; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int NSL, bool DL>
+__device__ __forceinline__ void finalize_row(const ApplyArgs& A, int row_block)
+{
+  const int lane = threadIdx.x % kFinalizeLanes;
+  const int s = row_block * kFinalizeRows + threadIdx.x / kFinalizeLanes;
+  // every lane of the warp takes part in the shuffles; rows past the end add zeros
+  const bool on = s < A.ne && !(A.active && *A.active == 0);
+  const int i = on ? A.perm[s] : 0;
+  const double scale = on ? A.trin[s].w * (0.25 / M_PI) : 0.0;
   const size_t stride = (size_t)A.nsplit * A.nitems;
+  const int nparts = A.nsplit * A.nchunk;
   for (int c = 0; c < NSL; ++c) {
-    double far = 0.0;
-    for (int sp = 0; sp < A.nsplit; ++sp)
-      for (int ch = 0; ch < A.nchunk; ++ch)
+    double far = 0.0, nr = 0.0;
+    if (on) {
+      for (int k = lane; k < nparts; k += kFinalizeLanes) {
+        const int sp = k / A.nchunk, ch = k - sp * A.nchunk;
         far += A.partial[c * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
-    double nr = 0.0;
-    for (int k = A.sl_rowptr[i]; k < A.sl_rowptr[i + 1]; ++k) nr += A.sl_val[k] * A.t[(size_t)c * A.tstride + A.sl_col[k]];
-    A.v[(size_t)c * A.vstride + i] = scale * far + nr;
+      }
+      for (int k = A.sl_rowptr[i] + lane; k < A.sl_rowptr[i + 1]; k += kFinalizeLanes)
+        nr += A.sl_val[k] * A.t[(size_t)c * A.tstride + A.sl_col[k]];
+    }
+    far = lanes_sum(far);
+    nr = lanes_sum(nr);
+    if (on && lane == 0) A.v[(size_t)c * A.vstride + i] = scale * far + nr;
   }
   if (DL) {
-    double far = 0.0;
-    for (int sp = 0; sp < A.nsplit; ++sp)
-      for (int ch = 0; ch < A.nchunk; ++ch)
+    double far = 0.0, nr = 0.0;
+    if (on) {
+      for (int k = lane; k < nparts; k += kFinalizeLanes) {
+        const int sp = k / A.nchunk, ch = k - sp * A.nchunk;
         far += A.partial[NSL * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
-    double nr = 0.0;
-    for (int k = A.dl_rowptr[i]; k < A.dl_rowptr[i + 1]; ++k) nr += A.dl_val[k] * A.u[A.dl_col[k]];
-    A.q[i] = scale * far + nr;
+      }
+      for (int k = A.dl_rowptr[i] + lane; k < A.dl_rowptr[i + 1]; k += kFinalizeLanes)
+        nr += A.dl_val[k] * A.u[A.dl_col[k]];
+    }
+    far = lanes_sum(far);
+    nr = lanes_sum(nr);
+    if (on && lane == 0) A.q[i] = scale * far + nr;
   }
 }
 
@@ -534,9 +559,9 @@ __global__ void prep_kernel(ApplyArgs A)
 }
 
 template <int NSL, bool DL>
-__global__ void finalize_kernel(ApplyArgs A)
+__global__ void __launch_bounds__(kFinalizeBlock) finalize_kernel(ApplyArgs A)
 {
-  finalize_row<NSL, DL>(A, blockIdx.x * blockDim.x + threadIdx.x);
+  finalize_row<NSL, DL>(A, blockIdx.x);
 }
 
 // Batched forms: block b belongs to entry e with off[e] <= b < off[e+1].
@@ -562,7 +587,7 @@ template <int NSL, bool DL>
 __global__ void finalize_batch_kernel(const ApplyArgs* __restrict__ args, const int* __restrict__ off, int n)
 {
   const int e = entry_of_block(off, n, blockIdx.x);
-  finalize_row<NSL, DL>(args[e], (blockIdx.x - off[e]) * blockDim.x + threadIdx.x);
+  finalize_row<NSL, DL>(args[e], blockIdx.x - off[e]);
 }
 
 // ---------------------------------------------------------------------------
@@ -695,10 +720,10 @@ cudaError_t prep_launch(bool fp32, int NSL, bool DL, const ApplyArgs& A, cudaStr
 
 cudaError_t finalize_launch(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st)
 {
-  const int blk = 128, grid = (A.ne + blk - 1) / blk;
+  const int grid = (A.ne + kFinalizeRows - 1) / kFinalizeRows;
 #define V(NS, D)                                                \
   if (NSL == NS && DL == D) {                                   \
-    finalize_kernel<NS, D><<<grid, blk, 0, st>>>(A);            \
+    finalize_kernel<NS, D><<<grid, kFinalizeBlock, 0, st>>>(A); \
     return cudaGetLastError();                                  \
   }
   EB_VARIANTS(V)

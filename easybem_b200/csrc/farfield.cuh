@@ -30,7 +30,10 @@
 
 namespace eb {
 
-constexpr int kTT = 128;  // target items (threads) per CTA
+#ifndef EB_TT
+#define EB_TT 128
+#endif
+constexpr int kTT = EB_TT;  // target items (threads) per CTA
 constexpr int kTS = 64;   // source triangles per shared-memory tile (Q <= 7)
 constexpr int kMaxRecSlots = 3;  // record slots of the widest variant
 constexpr int kMaxOutputs = 5;   // SL charges + DL of the widest variant
@@ -41,7 +44,9 @@ __host__ __device__ constexpr size_t far_smem_bytes(int src_tile, int Q, int nre
   return (size_t)src_tile * Q * nrec * (fp32 ? 16 : 32);
 }
 constexpr int kPrepBlock = 256;     // threads per block of the record preparation (one source point each)
-constexpr int kFinalizeBlock = 128; // threads per block of the finalize (one output row each)
+constexpr int kFinalizeBlock = 128; // threads per block of the finalize
+constexpr int kFinalizeLanes = 4;   // threads per output row (partial sums and CSR entries split over them)
+constexpr int kFinalizeRows = kFinalizeBlock / kFinalizeLanes;  // output rows per finalize block
 
 // FP64 record slot (two 16-byte halves).
 struct __align__(16) dq {

@@ -49,6 +49,11 @@ int eb_mesh_destroy(eb_mesh mesh);
  * regular quadrature-point pairs one far-field apply evaluates. */
 int eb_mesh_info(eb_mesh mesh, int* nnodes, int* nelems, long long* near_pairs,
                  long long* far_quad_pairs);
+/* Algorithmic bytes one SL+DL finalize launch moves (near-field CSR, the
+ * gathered densities, the far-field partial sums under the current plan and
+ * the outputs): the numerator of its HBM roofline. No counterpart in the
+ * reference. */
+int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes);
 
 /* v = V t, the P0 single layer (Galerkin, kernel 1/(4 pi |x-y|)); t and v
  * have nelems entries, host memory. Replaces applyGPULaplace3d1Layer(t, v, 0)
