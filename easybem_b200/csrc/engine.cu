@@ -246,9 +246,9 @@ static int build_near(Mesh* m)
 
 // Source triangles per shared-memory tile for a variant (whole cells when
 // they fit; large quadrature rules fall back to smaller tiles).
-int src_tile_for(int Q, bool fp32, int nsl, bool dl)
+int src_tile_for(int Q, bool fp32, int nsl, int nd)
 {
-  const size_t per_tri = far_smem_bytes(1, Q, rec_slots(nsl, dl), fp32);
+  const size_t per_tri = far_smem_bytes(1, Q, rec_slots(nsl, nd), fp32);
   const size_t budget = 48 * 1024;
   int ts = (int)std::min<size_t>(kTS, budget / per_tri);
   return std::max(ts, 1);
@@ -328,6 +328,7 @@ ApplyArgs mesh_apply_args(const Mesh* m, bool fp32, void* rec, const double* par
   A.t = t;
   A.tstride = tstride;
   A.u = u;
+  A.ustride = h.nv;  // DL columns [nd][nnodes]
   A.rec = rec;
   A.ne = h.ne;
   A.Q = h.Q;
@@ -346,11 +347,12 @@ ApplyArgs mesh_apply_args(const Mesh* m, bool fp32, void* rec, const double* par
   A.v = v;
   A.vstride = vstride;
   A.q = q;
+  A.qstride = h.ne;  // DL outputs [nd][nelems]
   A.active = nullptr;
   return A;
 }
 
-FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec, double* partial)
+FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, double* partial)
 {
   const HostMesh& h = m->h;
   FarMeshDesc desc;
@@ -373,33 +375,34 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec,
   desc.ne = h.ne;
   desc.Q = h.Q;
   desc.nsplit = m->plan.nsplit;
-  desc.src_tile = src_tile_for(h.Q, fp32, nsl, dl);
+  desc.src_tile = src_tile_for(h.Q, fp32, nsl, nd);
   if (m->plan.tile > 0) desc.src_tile = std::min(desc.src_tile, m->plan.tile);
   desc.active = nullptr;
   return desc;
 }
 
-int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
+int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const double* d_u, double* d_v,
                double* d_q, cudaStream_t st)
 {
+  const bool dl = nd > 0;
   HostMesh& h = m->h;
   const bool fp32 = precision == EB_PREC_MIXED;
   if (precision != EB_PREC_MIXED && precision != EB_PREC_FP64)
     return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
-  if (!far_variant_supported(nsl, dl)) return set_error(EB_ERR_INVALID, "unsupported operator combination");
+  if (!far_variant_supported(nsl, nd)) return set_error(EB_ERR_INVALID, "unsupported operator combination");
   if ((nsl > 0 && (!d_t || !d_v)) || (dl && (!d_u || !d_q))) return set_error(EB_ERR_INVALID, "null vector");
-  const int nrec = rec_slots(nsl, dl);
+  const int nrec = rec_slots(nsl, nd);
   // Scratch sized once for the largest variant, so device pointers captured
   // in descriptors (and in CUDA graphs) stay valid.
   if (!m->rec.p) {
     EB_CHECK(m->rec.alloc((size_t)h.ne * h.Q * kMaxRecSlots * sizeof(dq)));
     EB_CHECK(m->partial.alloc(sizeof(double) * (size_t)kMaxOutputs * m->plan.nsplit * h.nitems));
   }
-  Mesh::Variant& var = m->variants[(fp32 ? 64 : 0) + nsl * 2 + (dl ? 1 : 0)];
+  Mesh::Variant& var = m->variants[(fp32 ? 64 : 0) + nsl * 5 + nd];
   if (!var.desc.p) {
-    const FarMeshDesc desc = mesh_far_desc(m, fp32, nsl, dl, m->rec.p, m->partial.as<double>());
+    const FarMeshDesc desc = mesh_far_desc(m, fp32, nsl, nd, m->rec.p, m->partial.as<double>());
     const size_t smem = far_smem_bytes(desc.src_tile, h.Q, nrec, fp32);
-    int occ = far_occupancy(fp32, nsl, dl, h.K, h.Q, smem);
+    int occ = far_occupancy(fp32, nsl, nd, h.K, h.Q, smem);
     if (occ < 1) occ = 1;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
@@ -410,7 +413,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
     var.src_tile = desc.src_tile;
   }
   const ApplyArgs A = mesh_apply_args(m, fp32, m->rec.p, m->partial.as<double>(), d_t, h.ne, d_u, d_v, h.ne, d_q);
-  EB_CUDA(prep_launch(fp32, nsl, dl, A, st));
+  EB_CUDA(prep_launch(fp32, nsl, nd, A, st));
   EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
   if (m->profile) {
     if (!m->ev0) {
@@ -420,13 +423,13 @@ int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, cons
     }
     EB_CUDA(cudaEventRecord(m->ev0, st));
   }
-  EB_CUDA(far_launch(fp32, nsl, dl, h.K, h.Q, var.desc.as<FarMeshDesc>(), m->items.as<WorkItem>(), m->nitems_work,
+  EB_CUDA(far_launch(fp32, nsl, nd, h.K, h.Q, var.desc.as<FarMeshDesc>(), m->items.as<WorkItem>(), m->nitems_work,
                      m->counter.as<int>(), var.smem, var.grid, st));
   m->plan.grid = var.grid;
   m->plan.smem = var.smem;
   m->plan.src_tile = var.src_tile;
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev1, st));
-  EB_CUDA(finalize_launch(nsl, dl, A, st));
+  EB_CUDA(finalize_launch(nsl, nd, A, st));
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev2, st));
   return EB_OK;
 }
@@ -566,20 +569,40 @@ int eb_apply_sl_dl(eb_mesh mesh, int precision, const double* t, const double* u
 int eb_dirichlet_rhs(eb_mesh mesh, int nrhs, const double* g, double* b)
 {
   if (!mesh || !g || !b || nrhs < 1) return set_error(EB_ERR_INVALID, "null argument");
-  const eb::HostMesh& h = mesh->m->h;
-  for (int c = 0; c < nrhs; c++) {
-    const double* gc = g + (size_t)c * h.nv;
-    double* bc = b + (size_t)c * h.ne;
-    EB_CHECK(eb_apply_dl_p1(mesh, EB_PREC_FP64, gc, bc));
-    // + (1/2) M g with M[i][node] = J_i / 6 (src/BEM3dLaplace.cpp:469-477)
-    for (int i = 0; i < h.ne; i++) {
-      const int* f = &h.elems[3 * i];
-      const eb::d3 p0 = eb::mk3(h.nodes[3 * f[0]], h.nodes[3 * f[0] + 1], h.nodes[3 * f[0] + 2]);
-      const eb::d3 p1 = eb::mk3(h.nodes[3 * f[1]], h.nodes[3 * f[1] + 1], h.nodes[3 * f[1] + 2]);
-      const eb::d3 p2 = eb::mk3(h.nodes[3 * f[2]], h.nodes[3 * f[2] + 1], h.nodes[3 * f[2] + 2]);
-      const eb::d3 n = eb::cross3(p1 - p0, p2 - p0);
-      const double J = std::sqrt(eb::dot3(n, n));
-      bc[i] += 0.5 * (J / 6.0) * (gc[f[0]] + gc[f[1]] + gc[f[2]]);
+  std::lock_guard<std::mutex> lk(mesh->lock);
+  eb::Mesh* m = mesh->m;
+  EB_CUDA(cudaSetDevice(m->device));
+  const eb::HostMesh& h = m->h;
+  cudaStream_t st = mesh->stream;
+  // K g in FP64, four data sets per pass (they share every distance and
+  // 1/r^3 evaluation); a single set, or the last one of an odd group, uses the
+  // one-column variant, groups of two or three are padded with zero columns
+  constexpr int kCols = 4;
+  eb::DevBuf du, dq;
+  EB_CHECK(du.alloc(sizeof(double) * kCols * (size_t)h.nv));
+  EB_CHECK(dq.alloc(sizeof(double) * kCols * (size_t)h.ne));
+  for (int c0 = 0; c0 < nrhs; c0 += kCols) {
+    const int nc = std::min(kCols, nrhs - c0);
+    const int nd = nc == 1 ? 1 : kCols;
+    if (nc < nd) EB_CUDA(cudaMemsetAsync(du.p, 0, sizeof(double) * nd * (size_t)h.nv, st));
+    EB_CUDA(cudaMemcpyAsync(du.p, g + (size_t)c0 * h.nv, sizeof(double) * nc * (size_t)h.nv, cudaMemcpyHostToDevice,
+                            st));
+    EB_CHECK(eb::mesh_apply(m, EB_PREC_FP64, 0, nd, nullptr, du.as<double>(), nullptr, dq.as<double>(), st));
+    EB_CUDA(cudaMemcpyAsync(b + (size_t)c0 * h.ne, dq.p, sizeof(double) * nc * (size_t)h.ne, cudaMemcpyDeviceToHost,
+                            st));
+  }
+  EB_CUDA(cudaStreamSynchronize(st));
+  // + (1/2) M g with M[i][node] = J_i / 6 (src/BEM3dLaplace.cpp:469-477)
+  for (int i = 0; i < h.ne; i++) {
+    const int* f = &h.elems[3 * i];
+    const eb::d3 p0 = eb::mk3(h.nodes[3 * f[0]], h.nodes[3 * f[0] + 1], h.nodes[3 * f[0] + 2]);
+    const eb::d3 p1 = eb::mk3(h.nodes[3 * f[1]], h.nodes[3 * f[1] + 1], h.nodes[3 * f[1] + 2]);
+    const eb::d3 p2 = eb::mk3(h.nodes[3 * f[2]], h.nodes[3 * f[2] + 1], h.nodes[3 * f[2] + 2]);
+    const eb::d3 n = eb::cross3(p1 - p0, p2 - p0);
+    const double J6 = 0.5 * std::sqrt(eb::dot3(n, n)) / 6.0;
+    for (int c = 0; c < nrhs; c++) {
+      const double* gc = g + (size_t)c * h.nv;
+      b[(size_t)c * h.ne + i] += J6 * (gc[f[0]] + gc[f[1]] + gc[f[2]]);
     }
   }
   return EB_OK;

@@ -11,15 +11,15 @@
 namespace eb {
 
 // p1t selects P1 test functions (three outputs per item; NSL = 1, no DL).
-cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
+cudaError_t far_launch(bool fp32, int NSL, int ND, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
                        int* dc, size_t smem, int grid, cudaStream_t st, bool p1t = false);
-int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem, bool p1t = false);
-bool far_variant_supported(int NSL, bool DL);
-cudaError_t prep_launch(bool fp32, int NSL, bool DL, const ApplyArgs& A, cudaStream_t st);
-cudaError_t finalize_launch(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st);
-cudaError_t prep_launch_batch(bool fp32, int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n,
+int far_occupancy(bool fp32, int NSL, int ND, int K, int Q, size_t smem, bool p1t = false);
+bool far_variant_supported(int NSL, int ND);
+cudaError_t prep_launch(bool fp32, int NSL, int ND, const ApplyArgs& A, cudaStream_t st);
+cudaError_t finalize_launch(int NSL, int ND, const ApplyArgs& A, cudaStream_t st);
+cudaError_t prep_launch_batch(bool fp32, int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n,
                               int nblocks, cudaStream_t st);
-cudaError_t finalize_launch_batch(int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
+cudaError_t finalize_launch_batch(int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
                                   cudaStream_t st);
 
 // Simple owning device buffer.
@@ -73,7 +73,7 @@ struct Mesh {
   int nitems_work = 0;
   FarPlan plan;
   // one immutable device descriptor and launch shape per far-field variant
-  // (key = fp32 * 64 + nsl * 2 + dl), so a queued launch never sees it change
+  // (key = fp32 * 64 + nsl * 5 + nd), so a queued launch never sees it change
   struct Variant {
     DevBuf desc;
     int grid = 0;
@@ -94,11 +94,12 @@ int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int orde
 ApplyArgs mesh_apply_args(const Mesh* m, bool fp32, void* rec, const double* partial, const double* t, int tstride,
                           const double* u, double* v, int vstride, double* q);
 // Source triangles per shared-memory tile of a far-field variant.
-int src_tile_for(int Q, bool fp32, int nsl, bool dl);
+int src_tile_for(int Q, bool fp32, int nsl, int nd);
 // Far-field descriptor of mesh m for the given scratch.
-FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, bool dl, void* rec, double* partial);
-// Device-pointer apply: t has nsl columns (stride ne), v likewise; u/q for DL.
-int mesh_apply(Mesh* m, int precision, int nsl, bool dl, const double* d_t, const double* d_u, double* d_v,
+FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, double* partial);
+// Device-pointer apply: t has nsl columns (stride ne), v likewise; u has nd
+// DL columns (stride nnodes), q likewise (stride ne).
+int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const double* d_u, double* d_v,
                double* d_q, cudaStream_t st);
 
 // u(x) = V t - W u at npts points (device arrays: pts [npts][3], t [nelems], u [nnodes]).

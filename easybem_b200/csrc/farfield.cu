@@ -93,17 +93,19 @@ __device__ __forceinline__ double rsq_f64(double x)
 // expanded |x - y|^2, d from the cell-relative plane offset (P0_j - c_cell).n_j
 // in the working precision); otherwise the shared-vertex mask and direct
 // differences.
-template <typename T, int K, int NQ, int NSL, bool DL, bool FAR>
+template <typename T, int K, int NQ, int NSL, int ND, bool FAR>
 __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restrict__ srec,
                                           const int4* __restrict__ svid, const dq* __restrict__ snrm,
                                           const typename Slot<T>::type* __restrict__ splane, int s0,
                                           int s1, int nq, int4 tv, const T (&x)[K], const T (&y)[K],
                                           const T (&z)[K], const T (&q2)[K], const T (&o)[3],
                                           const double (&cen)[3], const double (&nrm)[3],
-                                          T (&sl)[NSL > 0 ? NSL : 1][K], T (&dl)[K])
+                                          T (&sl)[NSL > 0 ? NSL : 1][K], T (&dl)[ND > 0 ? ND : 1][K])
 {
   using S = typename Slot<T>::type;
-  constexpr int NREC = rec_slots(NSL, DL);
+  constexpr bool DL = ND > 0;
+  constexpr int NDX = ND > 0 ? ND : 1;
+  constexpr int NREC = rec_slots(NSL, ND);
   constexpr int kUnroll = std::is_same<T, float>::value ? kUnrollF32 : kUnrollF64;
   const int nqr = NQ > 0 ? NQ : nq;
 #pragma unroll 1
@@ -112,9 +114,11 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
       if (shares_vertex(tv, svid[s])) continue;
     }
     const S* r = srec + (size_t)s * nqr * NREC;
-    T acc[K];
+    T acc[NDX][K];
 #pragma unroll
-    for (int a = 0; a < K; ++a) acc[a] = 0;
+    for (int a = 0; a < K; ++a)
+#pragma unroll
+      for (int c = 0; c < NDX; ++c) acc[c][a] = 0;
 #pragma unroll(NQ > 0 ? (kUnroll > 0 ? kUnroll : NQ) : 1)
     for (int b = 0; b < nqr; ++b) {
       const S p0 = r[b * NREC];
@@ -133,11 +137,16 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
         else inv = rsq_f64(r2);
 #pragma unroll
         for (int c = 0; c < NSL; ++c) {
-          constexpr bool dlc = DL;
-          const int slot = charge_slot(c, dlc);
-          sl[c][a] += comp(slot == 1 ? p1 : r[b * NREC + slot], charge_comp(c, dlc)) * inv;
+          const int slot = charge_slot(c, ND);
+          sl[c][a] += comp(slot == 1 ? p1 : r[b * NREC + slot], charge_comp(c, ND)) * inv;
         }
-        if constexpr (DL) acc[a] += (inv * inv) * (p1.x * inv);
+        if constexpr (ND == 1) {
+          acc[0][a] += (inv * inv) * (p1.x * inv);
+        } else if constexpr (ND > 1) {
+          const T inv3 = (inv * inv) * inv;
+#pragma unroll
+          for (int c = 0; c < ND; ++c) acc[c][a] += comp(p1, c) * inv3;
+        }
       }
     }
     if constexpr (DL && FAR) {
@@ -146,7 +155,8 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
 #pragma unroll
       for (int a = 0; a < K; ++a) {
         const T d = x[a] * pn.x + (y[a] * pn.y + (z[a] * pn.z - pn.w));
-        dl[a] += d * acc[a];
+#pragma unroll
+        for (int c = 0; c < ND; ++c) dl[c][a] += d * acc[c][a];
       }
     } else if constexpr (DL) {
       // x_a - c_i = (x_a - c_cell) + o with o = c_cell - c_i
@@ -156,7 +166,8 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
 #pragma unroll
       for (int a = 0; a < K; ++a) {
         const T d = x[a] * dnx + (y[a] * dny + (z[a] * dnz + e));
-        dl[a] += d * acc[a];
+#pragma unroll
+        for (int c = 0; c < ND; ++c) dl[c][a] += d * acc[c][a];
       }
     }
   }
@@ -173,29 +184,32 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
 // FMA-pipe work per quadrature pair is unchanged (FFMA2 occupies the pipe
 // for two lanes' worth); the pair form halves the issue slots, which bound
 // the scalar loop.
-template <int K, int NQ, int NSL, bool DL, bool FAR>
+template <int K, int NQ, int NSL, int ND, bool FAR>
 __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, const int4* __restrict__ svid,
                                              const dq* __restrict__ snrm, const float4* __restrict__ splane, int s0,
                                              int s1, int nq, int4 tv, const float (&x)[K], const float (&y)[K],
                                              const float (&z)[K], const float (&q2)[K], const float (&o)[3],
                                              const double (&cen)[3], const double (&nrm)[3],
-                                             float (&sl)[NSL > 0 ? NSL : 1][K], float (&dl)[K])
+                                             float (&sl)[NSL > 0 ? NSL : 1][K], float (&dl)[ND > 0 ? ND : 1][K])
 {
-  constexpr int NREC = rec_slots(NSL, DL);
+  constexpr bool DL = ND > 0;
+  constexpr int NDX = ND > 0 ? ND : 1;
+  constexpr int NREC = rec_slots(NSL, ND);
   constexpr int NS = NSL > 0 ? NSL : 1;
   constexpr int KP = K / 2;           // packed target pairs
   constexpr int KP1 = KP > 0 ? KP : 1;
   constexpr bool ODD = (K & 1) != 0;  // last target point runs scalar
   constexpr int PS = 4 * NREC;        // staged floats per source point
   const int nqr = NQ > 0 ? NQ : nq;
-  float2 X[KP1], Y[KP1], Z[KP1], W[KP1], SL[NS][KP1], DLp[KP1];
+  float2 X[KP1], Y[KP1], Z[KP1], W[KP1], SL[NS][KP1], DLp[NDX][KP1];
 #pragma unroll
   for (int p = 0; p < KP; ++p) {
     X[p] = make_float2(x[2 * p], x[2 * p + 1]);
     Y[p] = make_float2(y[2 * p], y[2 * p + 1]);
     Z[p] = make_float2(z[2 * p], z[2 * p + 1]);
     W[p] = make_float2(q2[2 * p], q2[2 * p + 1]);
-    DLp[p] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < NDX; ++c) DLp[c][p] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int c = 0; c < NS; ++c) SL[c][p] = make_float2(0.f, 0.f);
   }
@@ -206,10 +220,14 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
       if (shares_vertex(tv, svid[s])) continue;
     }
     const float* r = srec + (size_t)s * nqr * PS;
-    float2 acc2[KP1];
-    float acc1 = 0.f;
+    float2 acc2[NDX][KP1];
+    float acc1[NDX];
 #pragma unroll
-    for (int p = 0; p < KP; ++p) acc2[p] = make_float2(0.f, 0.f);
+    for (int c = 0; c < NDX; ++c) {
+      acc1[c] = 0.f;
+#pragma unroll
+      for (int p = 0; p < KP; ++p) acc2[c][p] = make_float2(0.f, 0.f);
+    }
 #pragma unroll(NQ > 0 ? (kUnrollX2 > 0 ? kUnrollX2 : NQ) : 1)
     for (int b = 0; b < nqr; ++b) {
       const float* rb = r + b * PS;
@@ -220,10 +238,15 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
       float2 ch[NS];
 #pragma unroll
       for (int c = 0; c < NSL; ++c) {
-        const float v = comp(rv[charge_slot(c, DL)], charge_comp(c, DL));
+        const float v = comp(rv[charge_slot(c, ND)], charge_comp(c, ND));
         ch[c] = make_float2(v, v);
       }
-      const float2 sdl = DL ? make_float2(rv[1].x, rv[1].x) : make_float2(0.f, 0.f);
+      float2 sd[NDX];
+#pragma unroll
+      for (int c = 0; c < NDX; ++c) {
+        const float v = DL ? comp(rv[1], c) : 0.f;
+        sd[c] = make_float2(v, v);
+      }
 #pragma unroll
       for (int p = 0; p < KP; ++p) {
         float2 r2;
@@ -238,7 +261,13 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
         const float2 inv = make_float2(rsq(r2.x), rsq(r2.y));
 #pragma unroll
         for (int c = 0; c < NSL; ++c) SL[c][p] = __ffma2_rn(ch[c], inv, SL[c][p]);
-        if constexpr (DL) acc2[p] = __ffma2_rn(__fmul2_rn(inv, inv), __fmul2_rn(sdl, inv), acc2[p]);
+        if constexpr (ND == 1) {
+          acc2[0][p] = __ffma2_rn(__fmul2_rn(inv, inv), __fmul2_rn(sd[0], inv), acc2[0][p]);
+        } else if constexpr (ND > 1) {
+          const float2 inv3 = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+#pragma unroll
+          for (int c = 0; c < ND; ++c) acc2[c][p] = __ffma2_rn(sd[c], inv3, acc2[c][p]);
+        }
       }
       if constexpr (ODD) {
         constexpr int a = K - 1;
@@ -252,7 +281,13 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
         const float inv = rsq(r2);
 #pragma unroll
         for (int c = 0; c < NSL; ++c) sl[c][a] += ch[c].x * inv;
-        if constexpr (DL) acc1 += (inv * inv) * (sdl.x * inv);
+        if constexpr (ND == 1) {
+          acc1[0] += (inv * inv) * (sd[0].x * inv);
+        } else if constexpr (ND > 1) {
+          const float inv3 = (inv * inv) * inv;
+#pragma unroll
+          for (int c = 0; c < ND; ++c) acc1[c] += sd[c].x * inv3;
+        }
       }
     }
     if constexpr (DL) {
@@ -271,12 +306,14 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
 #pragma unroll
       for (int p = 0; p < KP; ++p) {
         const float2 d = __ffma2_rn(X[p], nx, __ffma2_rn(Y[p], ny, __ffma2_rn(Z[p], nz, nw)));
-        DLp[p] = __ffma2_rn(d, acc2[p], DLp[p]);
+#pragma unroll
+        for (int c = 0; c < ND; ++c) DLp[c][p] = __ffma2_rn(d, acc2[c][p], DLp[c][p]);
       }
       if constexpr (ODD) {
         constexpr int a = K - 1;
         const float d = x[a] * pnx + (y[a] * pny + (z[a] * pnz + pnw));
-        dl[a] += d * acc1;
+#pragma unroll
+        for (int c = 0; c < ND; ++c) dl[c][a] += d * acc1[c];
       }
     }
   }
@@ -287,23 +324,28 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
       sl[c][2 * p] += SL[c][p].x;
       sl[c][2 * p + 1] += SL[c][p].y;
     }
-    dl[2 * p] += DLp[p].x;
-    dl[2 * p + 1] += DLp[p].y;
+#pragma unroll
+    for (int c = 0; c < ND; ++c) {
+      dl[c][2 * p] += DLp[c][p].x;
+      dl[c][2 * p + 1] += DLp[c][p].y;
+    }
   }
 }
 
 // P1T: P1 test functions; the item's three outputs are sum_a w_a phi_k(x_a) acc_a
 // (k = 0, 1, 2 in the triangle's vertex order) of the single SL charge.
-template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
+template <typename T, int K, int NQ, int NSL, int ND, bool P1T>
 __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MINB : EB_F64_MINB)
     far_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
                int* __restrict__ counter)
 {
   using S = typename Slot<T>::type;
   constexpr bool F32 = std::is_same<T, float>::value;
-  constexpr int NREC = rec_slots(NSL, DL);
+  constexpr bool DL = ND > 0;
+  constexpr int NDX = ND > 0 ? ND : 1;
+  constexpr int NREC = rec_slots(NSL, ND);
   constexpr int NS = NSL > 0 ? NSL : 1;
-  constexpr int NACC = P1T ? 3 : NS + 1;
+  constexpr int NACC = P1T ? 3 : NS + NDX;
   static_assert(!P1T || (NSL == 1 && !DL), "P1 test functions pair with one SL charge");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_item;
@@ -392,27 +434,28 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
             xs[a] = px - o[0]; ys[a] = py - o[1]; zs[a] = pz - o[2];
             q2[a] = xs[a] * xs[a] + ys[a] * ys[a] + zs[a] * zs[a];
           }
-          T sl[NS][K], dl[K];
+          T sl[NS][K], dl[NDX][K];
 #pragma unroll
           for (int a = 0; a < K; ++a) {
-            dl[a] = 0;
+#pragma unroll
+            for (int c = 0; c < NDX; ++c) dl[c][a] = 0;
 #pragma unroll
             for (int c = 0; c < NS; ++c) sl[c][a] = 0;
           }
           if constexpr (F32) {
             const float* sf = reinterpret_cast<const float*>(s_rec);
             if (far)
-              eval_cell_x2<K, NQ, NSL, DL, true>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+              eval_cell_x2<K, NQ, NSL, ND, true>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
                                                  nrm, sl, dl);
             else
-              eval_cell_x2<K, NQ, NSL, DL, false>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+              eval_cell_x2<K, NQ, NSL, ND, false>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
                                                   nrm, sl, dl);
           } else {
             if (far)
-              eval_cell<T, K, NQ, NSL, DL, true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
+              eval_cell<T, K, NQ, NSL, ND, true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
                                                  cen, nrm, sl, dl);
             else
-              eval_cell<T, K, NQ, NSL, DL, false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
+              eval_cell<T, K, NQ, NSL, ND, false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
                                                   cen, nrm, sl, dl);
           }
           if constexpr (P1T) {
@@ -430,16 +473,17 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
               else acc_hi[k] += part;
             }
           } else {
+            // accumulator c < NS: SL charge c; NS + c: DL column c
 #pragma unroll
-            for (int c = 0; c <= NS; ++c) {
-              if (c == NS && !DL) break;
+            for (int c = 0; c < NS + NDX; ++c) {
+              if (c >= NS + ND) break;
               if (c < NS && NSL == 0) continue;
               T part = 0;
 #pragma unroll
               for (int a = 0; a < K; ++a) {
                 T px, py, pz, pw;
                 target(a, px, py, pz, pw);
-                part += pw * (c < NS ? sl[c][a] : dl[a]);
+                part += pw * (c < NS ? sl[c][a] : dl[c - NS][a]);
               }
               if constexpr (F32) two_sum_add(acc_hi[c], acc_lo[c], part);
               else acc_hi[c] += part;
@@ -459,19 +503,21 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
       } else {
 #pragma unroll
         for (int c = 0; c < NSL; ++c) out[c * stride] = (double)acc_hi[c] + (double)acc_lo[c];
-        if (DL) out[NSL * stride] = (double)acc_hi[NS] + (double)acc_lo[NS];
+#pragma unroll
+        for (int c = 0; c < ND; ++c) out[(NSL + c) * stride] = (double)acc_hi[NS + c] + (double)acc_lo[NS + c];
       }
     }
   }
 }
 
 // Source records for one apply: positions (static) with the per-apply
-// strengths s = w_b J_j u_h(y_b) (DL) and charges c_r = w_b J_j t_r[j] (SL).
-template <typename T, int NSL, bool DL>
+// strengths s_c = w_b J_j u_h,c(y_b) (DL column c) and charges
+// c_r = w_b J_j t_r[j] (SL).
+template <typename T, int NSL, int ND>
 __device__ __forceinline__ void prep_point(const ApplyArgs& A, long long idx)
 {
   using S = typename Slot<T>::type;
-  constexpr int NREC = rec_slots(NSL, DL);
+  constexpr int NREC = rec_slots(NSL, ND);
   if (idx >= (long long)A.ne * A.Q || (A.active && *A.active == 0)) return;
   const int j = (int)(idx / A.Q), b = (int)(idx % A.Q);
   const double wj = A.wj[idx];  // w_b * J_j
@@ -481,12 +527,16 @@ __device__ __forceinline__ void prep_point(const ApplyArgs& A, long long idx)
   for (int k = 0; k < 4 * NREC; ++k) vals[k] = 0;
 #pragma unroll
   for (int c = 0; c < NSL; ++c)
-    vals[4 * charge_slot(c, DL) + charge_comp(c, DL)] = (T)(wj * A.t[(size_t)c * A.tstride + orig]);
-  if constexpr (DL) {
+    vals[4 * charge_slot(c, ND) + charge_comp(c, ND)] = (T)(wj * A.t[(size_t)c * A.tstride + orig]);
+  if constexpr (ND > 0) {
     const int4 v = A.svid[j];
     const double e1 = A.bary[2 * b], e2 = A.bary[2 * b + 1];
-    const double uh = (1.0 - e1 - e2) * A.u[v.x] + e1 * A.u[v.y] + e2 * A.u[v.z];
-    vals[4] = (T)(wj * uh);
+#pragma unroll
+    for (int c = 0; c < ND; ++c) {
+      const double* u = A.u + (size_t)c * A.ustride;
+      const double uh = (1.0 - e1 - e2) * u[v.x] + e1 * u[v.y] + e2 * u[v.z];
+      vals[4 + c] = (T)(wj * uh);
+    }
   }
   S* r = reinterpret_cast<S*>(A.rec) + idx * NREC;
   r[0] = reinterpret_cast<const S*>(A.pos)[idx];
@@ -511,7 +561,7 @@ __device__ __forceinline__ double lanes_sum(double v)
   return v;
 }
 
-template <int NSL, bool DL>
+template <int NSL, int ND>
 __device__ __forceinline__ void finalize_row(const ApplyArgs& A, int row_block)
 {
   const int lane = threadIdx.x % kFinalizeLanes;
@@ -536,32 +586,33 @@ __device__ __forceinline__ void finalize_row(const ApplyArgs& A, int row_block)
     nr = lanes_sum(nr);
     if (on && lane == 0) A.v[(size_t)c * A.vstride + i] = scale * far + nr;
   }
-  if (DL) {
+  for (int c = 0; c < ND; ++c) {
     double far = 0.0, nr = 0.0;
     if (on) {
       for (int k = lane; k < nparts; k += kFinalizeLanes) {
         const int sp = k / A.nchunk, ch = k - sp * A.nchunk;
-        far += A.partial[NSL * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
+        far += A.partial[(NSL + c) * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
       }
+      const double* u = A.u + (size_t)c * A.ustride;
       for (int k = A.dl_rowptr[i] + lane; k < A.dl_rowptr[i + 1]; k += kFinalizeLanes)
-        nr += A.dl_val[k] * A.u[A.dl_col[k]];
+        nr += A.dl_val[k] * u[A.dl_col[k]];
     }
     far = lanes_sum(far);
     nr = lanes_sum(nr);
-    if (on && lane == 0) A.q[i] = scale * far + nr;
+    if (on && lane == 0) A.q[(size_t)c * A.qstride + i] = scale * far + nr;
   }
 }
 
-template <typename T, int NSL, bool DL>
+template <typename T, int NSL, int ND>
 __global__ void prep_kernel(ApplyArgs A)
 {
-  prep_point<T, NSL, DL>(A, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  prep_point<T, NSL, ND>(A, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-template <int NSL, bool DL>
+template <int NSL, int ND>
 __global__ void __launch_bounds__(kFinalizeBlock) finalize_kernel(ApplyArgs A)
 {
-  finalize_row<NSL, DL>(A, blockIdx.x);
+  finalize_row<NSL, ND>(A, blockIdx.x);
 }
 
 // Batched forms: block b belongs to entry e with off[e] <= b < off[e+1].
@@ -576,18 +627,18 @@ __device__ __forceinline__ int entry_of_block(const int* __restrict__ off, int n
   return lo;
 }
 
-template <typename T, int NSL, bool DL>
+template <typename T, int NSL, int ND>
 __global__ void prep_batch_kernel(const ApplyArgs* __restrict__ args, const int* __restrict__ off, int n)
 {
   const int e = entry_of_block(off, n, blockIdx.x);
-  prep_point<T, NSL, DL>(args[e], (long long)(blockIdx.x - off[e]) * blockDim.x + threadIdx.x);
+  prep_point<T, NSL, ND>(args[e], (long long)(blockIdx.x - off[e]) * blockDim.x + threadIdx.x);
 }
 
-template <int NSL, bool DL>
+template <int NSL, int ND>
 __global__ void finalize_batch_kernel(const ApplyArgs* __restrict__ args, const int* __restrict__ off, int n)
 {
   const int e = entry_of_block(off, n, blockIdx.x);
-  finalize_row<NSL, DL>(args[e], blockIdx.x - off[e]);
+  finalize_row<NSL, ND>(args[e], blockIdx.x - off[e]);
 }
 
 // ---------------------------------------------------------------------------
@@ -596,14 +647,14 @@ __global__ void finalize_batch_kernel(const ApplyArgs* __restrict__ args, const 
 struct FarLaunch {
   bool fp32;
   int K, NQ, NSL;
-  bool DL;
+  int ND;
 };
 
-template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
+template <typename T, int K, int NQ, int NSL, int ND, bool P1T>
 static cudaError_t launch_far_t(const FarMeshDesc* d_meshes, const WorkItem* d_items, int nitems, int* d_counter,
                                 size_t smem, int grid, cudaStream_t st)
 {
-  auto kern = far_kernel<T, K, NQ, NSL, DL, P1T>;
+  auto kern = far_kernel<T, K, NQ, NSL, ND, P1T>;
   // the kernel's static shared memory (up to ~4 KB) counts against the same
   // 48 KB default, so opt in above 32 KB of dynamic shared memory
   if (smem > 32 * 1024) {
@@ -614,97 +665,100 @@ static cudaError_t launch_far_t(const FarMeshDesc* d_meshes, const WorkItem* d_i
   return cudaGetLastError();
 }
 
-template <typename T, int K, int NQ, int NSL, bool DL, bool P1T>
+template <typename T, int K, int NQ, int NSL, int ND, bool P1T>
 static int occupancy_t(size_t smem)
 {
   int nb = 0;
   if (smem > 32 * 1024)
-    cudaFuncSetAttribute(far_kernel<T, K, NQ, NSL, DL, P1T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_kernel<T, K, NQ, NSL, DL, P1T>, kTT, smem);
+    cudaFuncSetAttribute(far_kernel<T, K, NQ, NSL, ND, P1T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, far_kernel<T, K, NQ, NSL, ND, P1T>, kTT, smem);
   return nb;
 }
 
 // (points per item K, rule size NQ; NQ = 0: rule size read at run time)
 #define EB_FAR_CASES(X) X(1, 1) X(3, 3) X(4, 4) X(6, 6) X(7, 7) X(8, 0)
 
-// Operator variants compiled: (SL charges, DL) for record preparation and
-// finalize; the far field adds the P1-test variant (1 charge, no DL).
-#define EB_VARIANTS(V) V(0, true) V(1, false) V(1, true) V(3, false) V(4, false)
+// Operator variants compiled, (SL charges, DL columns), for record
+// preparation, far field and finalize: the fused SL+DL apply, SL alone with
+// 1, 3 or 4 right-hand sides, DL alone with 1 or 4 densities (4: the
+// Dirichlet right-hand sides of multi-RHS solves); the far field adds the
+// P1-test variant (1 charge, no DL).
+#define EB_VARIANTS(V) V(0, 1) V(1, 0) V(1, 1) V(3, 0) V(4, 0) V(0, 4)
 #define EB_FAR_VARIANTS(V) \
-  V(0, true, false) V(1, false, false) V(1, true, false) V(3, false, false) V(4, false, false) V(1, false, true)
+  V(0, 1, false) V(1, 0, false) V(1, 1, false) V(3, 0, false) V(4, 0, false) V(1, 0, true) V(0, 4, false)
 
-template <typename T, int NSL, bool DL, bool P1T>
+template <typename T, int NSL, int ND, bool P1T>
 static cudaError_t dispatch_k(int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, size_t smem,
                               int grid, cudaStream_t st)
 {
 #define X(KK, NQQ)                                    \
   if (K == KK && (NQQ == 0 || Q == NQQ))              \
-    return launch_far_t<T, KK, NQQ, NSL, DL, P1T>(dm, di, n, dc, smem, grid, st);
+    return launch_far_t<T, KK, NQQ, NSL, ND, P1T>(dm, di, n, dc, smem, grid, st);
   EB_FAR_CASES(X)
 #undef X
   return cudaErrorInvalidValue;
 }
 
-template <typename T, int NSL, bool DL, bool P1T>
+template <typename T, int NSL, int ND, bool P1T>
 static int dispatch_occ(int K, int Q, size_t smem)
 {
 #define X(KK, NQQ) \
-  if (K == KK && (NQQ == 0 || Q == NQQ)) return occupancy_t<T, KK, NQQ, NSL, DL, P1T>(smem);
+  if (K == KK && (NQQ == 0 || Q == NQQ)) return occupancy_t<T, KK, NQQ, NSL, ND, P1T>(smem);
   EB_FAR_CASES(X)
 #undef X
   return 0;
 }
 
 template <typename T>
-static cudaError_t far_launch_t(int NSL, bool DL, bool P1, int K, int Q, const FarMeshDesc* dm, const WorkItem* di,
+static cudaError_t far_launch_t(int NSL, int ND, bool P1, int K, int Q, const FarMeshDesc* dm, const WorkItem* di,
                                 int n, int* dc, size_t smem, int grid, cudaStream_t st)
 {
 #define V(NS, D, P) \
-  if (NSL == NS && DL == D && P1 == P) return dispatch_k<T, NS, D, P>(K, Q, dm, di, n, dc, smem, grid, st);
+  if (NSL == NS && ND == D && P1 == P) return dispatch_k<T, NS, D, P>(K, Q, dm, di, n, dc, smem, grid, st);
   EB_FAR_VARIANTS(V)
 #undef V
   return cudaErrorInvalidValue;
 }
 
 template <typename T>
-static int far_occ_t(int NSL, bool DL, bool P1, int K, int Q, size_t smem)
+static int far_occ_t(int NSL, int ND, bool P1, int K, int Q, size_t smem)
 {
 #define V(NS, D, P) \
-  if (NSL == NS && DL == D && P1 == P) return dispatch_occ<T, NS, D, P>(K, Q, smem);
+  if (NSL == NS && ND == D && P1 == P) return dispatch_occ<T, NS, D, P>(K, Q, smem);
   EB_FAR_VARIANTS(V)
 #undef V
   return 0;
 }
 
-bool far_variant_supported(int NSL, bool DL)
+bool far_variant_supported(int NSL, int ND)
 {
 #define V(NS, D) \
-  if (NSL == NS && DL == D) return true;
+  if (NSL == NS && ND == D) return true;
   EB_VARIANTS(V)
 #undef V
   return false;
 }
 
-cudaError_t far_launch(bool fp32, int NSL, bool DL, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
+cudaError_t far_launch(bool fp32, int NSL, int ND, int K, int Q, const FarMeshDesc* dm, const WorkItem* di, int n,
                        int* dc, size_t smem, int grid, cudaStream_t st, bool p1t)
 {
-  return fp32 ? far_launch_t<float>(NSL, DL, p1t, K, Q, dm, di, n, dc, smem, grid, st)
-              : far_launch_t<double>(NSL, DL, p1t, K, Q, dm, di, n, dc, smem, grid, st);
+  return fp32 ? far_launch_t<float>(NSL, ND, p1t, K, Q, dm, di, n, dc, smem, grid, st)
+              : far_launch_t<double>(NSL, ND, p1t, K, Q, dm, di, n, dc, smem, grid, st);
 }
 
-int far_occupancy(bool fp32, int NSL, bool DL, int K, int Q, size_t smem, bool p1t)
+int far_occupancy(bool fp32, int NSL, int ND, int K, int Q, size_t smem, bool p1t)
 {
-  return fp32 ? far_occ_t<float>(NSL, DL, p1t, K, Q, smem) : far_occ_t<double>(NSL, DL, p1t, K, Q, smem);
+  return fp32 ? far_occ_t<float>(NSL, ND, p1t, K, Q, smem) : far_occ_t<double>(NSL, ND, p1t, K, Q, smem);
 }
 
 template <typename T>
-static cudaError_t prep_launch_t(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st)
+static cudaError_t prep_launch_t(int NSL, int ND, const ApplyArgs& A, cudaStream_t st)
 {
   const long long n = (long long)A.ne * A.Q;
   const int blk = 256;
   const int grid = (int)((n + blk - 1) / blk);
 #define V(NS, D)                                                \
-  if (NSL == NS && DL == D) {                                   \
+  if (NSL == NS && ND == D) {                                   \
     prep_kernel<T, NS, D><<<grid, blk, 0, st>>>(A);             \
     return cudaGetLastError();                                  \
   }
@@ -713,16 +767,16 @@ static cudaError_t prep_launch_t(int NSL, bool DL, const ApplyArgs& A, cudaStrea
   return cudaErrorInvalidValue;
 }
 
-cudaError_t prep_launch(bool fp32, int NSL, bool DL, const ApplyArgs& A, cudaStream_t st)
+cudaError_t prep_launch(bool fp32, int NSL, int ND, const ApplyArgs& A, cudaStream_t st)
 {
-  return fp32 ? prep_launch_t<float>(NSL, DL, A, st) : prep_launch_t<double>(NSL, DL, A, st);
+  return fp32 ? prep_launch_t<float>(NSL, ND, A, st) : prep_launch_t<double>(NSL, ND, A, st);
 }
 
-cudaError_t finalize_launch(int NSL, bool DL, const ApplyArgs& A, cudaStream_t st)
+cudaError_t finalize_launch(int NSL, int ND, const ApplyArgs& A, cudaStream_t st)
 {
   const int grid = (A.ne + kFinalizeRows - 1) / kFinalizeRows;
 #define V(NS, D)                                                \
-  if (NSL == NS && DL == D) {                                   \
+  if (NSL == NS && ND == D) {                                   \
     finalize_kernel<NS, D><<<grid, kFinalizeBlock, 0, st>>>(A); \
     return cudaGetLastError();                                  \
   }
@@ -732,11 +786,11 @@ cudaError_t finalize_launch(int NSL, bool DL, const ApplyArgs& A, cudaStream_t s
 }
 
 template <typename T>
-static cudaError_t prep_batch_t(int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
+static cudaError_t prep_batch_t(int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
                                 cudaStream_t st)
 {
 #define V(NS, D)                                                                  \
-  if (NSL == NS && DL == D) {                                                     \
+  if (NSL == NS && ND == D) {                                                     \
     prep_batch_kernel<T, NS, D><<<nblocks, kPrepBlock, 0, st>>>(d_args, d_off, n); \
     return cudaGetLastError();                                                    \
   }
@@ -745,18 +799,18 @@ static cudaError_t prep_batch_t(int NSL, bool DL, const ApplyArgs* d_args, const
   return cudaErrorInvalidValue;
 }
 
-cudaError_t prep_launch_batch(bool fp32, int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n,
+cudaError_t prep_launch_batch(bool fp32, int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n,
                               int nblocks, cudaStream_t st)
 {
-  return fp32 ? prep_batch_t<float>(NSL, DL, d_args, d_off, n, nblocks, st)
-              : prep_batch_t<double>(NSL, DL, d_args, d_off, n, nblocks, st);
+  return fp32 ? prep_batch_t<float>(NSL, ND, d_args, d_off, n, nblocks, st)
+              : prep_batch_t<double>(NSL, ND, d_args, d_off, n, nblocks, st);
 }
 
-cudaError_t finalize_launch_batch(int NSL, bool DL, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
+cudaError_t finalize_launch_batch(int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
                                   cudaStream_t st)
 {
 #define V(NS, D)                                                                          \
-  if (NSL == NS && DL == D) {                                                             \
+  if (NSL == NS && ND == D) {                                                             \
     finalize_batch_kernel<NS, D><<<nblocks, kFinalizeBlock, 0, st>>>(d_args, d_off, n);   \
     return cudaGetLastError();                                                            \
   }

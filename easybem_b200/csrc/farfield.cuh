@@ -55,15 +55,17 @@ struct __align__(16) dq {
 
 // Source-point record layout (FP32: float4 slots, FP64: dq slots):
 //   slot0 = (-2 y, |y|^2), y the quadrature point relative to its cell centre;
-//   slot1.. = the strengths [s (with DL), c_0, c_1, ...], four per slot, where
+//   slot1.. = the strengths [s_0 .. s_{nd-1} (DL columns), c_0, c_1, ...], four
+//   per slot, where
 //   c_r = w_b J_j t_r[j] are the SL charges and s = w_b J_j u_h(y_b) the DL
 //   strength. Far cells use |x - y|^2 = |x|^2 + |y|^2 - 2 x.y directly from
 //   slot0; near cells recover y = -(1/2)(-2y) exactly.
-__host__ __device__ constexpr int rec_slots(int nsl, bool dl) { return 1 + (nsl + (dl ? 1 : 0) + 3) / 4; }
+__host__ __device__ constexpr int rec_slots(int nsl, int nd) { return 1 + (nsl + nd + 3) / 4; }
 
-// Slot and component of SL charge r (the DL strength is slot 1, component 0).
-__host__ __device__ constexpr int charge_slot(int r, bool dl) { return 1 + (r + (dl ? 1 : 0)) / 4; }
-__host__ __device__ constexpr int charge_comp(int r, bool dl) { return (r + (dl ? 1 : 0)) % 4; }
+// Slot and component of SL charge r after nd DL strengths (DL strength c is
+// slot 1 + c / 4, component c % 4).
+__host__ __device__ constexpr int charge_slot(int r, int nd) { return 1 + (r + nd) / 4; }
+__host__ __device__ constexpr int charge_comp(int r, int nd) { return (r + nd) % 4; }
 
 // A source cell is "far" from a target tile when the distance of their
 // bounding-sphere centres exceeds kFarRatio times the sum of the radii (which
@@ -107,7 +109,8 @@ struct ApplyArgs {
   const double* bary;    // triangle-rule points (eta1, eta2)
   const double* t;       // SL densities, nsl columns of stride tstride
   int tstride;
-  const double* u;       // DL density (vertex values)
+  const double* u;       // DL densities (vertex values), nd columns of stride ustride
+  int ustride;
   void* rec;             // records out
   int ne, Q;
   // finalize
@@ -123,7 +126,8 @@ struct ApplyArgs {
   const double* dl_val;
   double* v;             // SL outputs, nsl columns of stride vstride
   int vstride;
-  double* q;             // DL output
+  double* q;             // DL outputs, nd columns of stride qstride
+  int qstride;
   const int* active;     // optional: skip this mesh while *active == 0
 };
 

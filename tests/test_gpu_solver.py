@@ -142,3 +142,23 @@ def test_preconditioner_matches_oracle_restatement(gpu_lib, oracle):
     VM = np.asarray(V) @ M
     ev = np.linalg.svd(VM, compute_uv=False)
     assert ev[0] / ev[-1] < np.linalg.cond(np.asarray(V)) / 3
+
+
+def test_dirichlet_rhs_several_data_sets(gpu_lib, oracle):
+    # 1, 2, 3 and 5 data sets: the one-column DL pass, a padded four-column
+    # pass, and a full four-column pass plus a single one, all against the
+    # oracle's dense K and M (FP64)
+    nodes, elems = meshes.perturbed_icosphere(2, seed=6)
+    oracle.set_order(4)
+    V, K = oracle.dense(nodes, elems)
+    M = _mass(nodes, elems)
+    rng = np.random.default_rng(10)
+    with gpu_lib.Mesh(nodes, elems) as m:
+        for n in (1, 2, 3, 5):
+            g = rng.normal(size=(n, nodes.shape[0]))
+            b = m.dirichlet_rhs(g)
+            ref = (0.5 * M @ g.T + np.asarray(K) @ g.T).T
+            assert b.shape == (n, elems.shape[0])
+            assert rel_l2(b, ref) < 1e-12, n
+            for k in range(n):
+                assert rel_l2(b[k], ref[k]) < 1e-12, (n, k)
