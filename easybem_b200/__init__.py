@@ -375,6 +375,16 @@ class Server:
         check(lib().eb_server_usage(self._h, ctypes.byref(u), ctypes.byref(b)))
         return u.value, b.value
 
+    STAT_NAMES = ("steps", "step_s", "rebuilds", "rebuild_s", "prepared", "prepare_s", "mesh_s", "rhs_s",
+                  "precond_s", "mesh_topology_s", "mesh_tables_s", "mesh_near_s")
+
+    def stats(self):
+        """Operating counters: steps and time in step(), solver batch rebuilds,
+        and the preparation worker's time (mesh, right-hand sides, preconditioner)."""
+        v = np.zeros(len(self.STAT_NAMES))
+        check(lib().eb_server_stats(self._h, _ptr(v), len(v)))
+        return dict(zip(self.STAT_NAMES, v.tolist()))
+
 
 def solve(problems, **options):
     """Solves V x = b for a list of (mesh, b) with b [ne] or [nrhs, ne], all in lockstep.

@@ -77,6 +77,7 @@ _SIGNATURES = {
     "eb_server_result": (ctypes.c_int, [_dp, ctypes.c_longlong, _dp, _dp, _dp]),
     "eb_server_release": (ctypes.c_int, [_dp, ctypes.c_longlong]),
     "eb_server_usage": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_server_stats": (ctypes.c_int, [_dp, _dp, ctypes.c_int]),
     "eb_last_kernel_ms": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "eb_mesh_set_plan": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int]),
     "eb_mesh_get_plan": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),

@@ -20,10 +20,13 @@ int batch_entry_init(BatchEntry* e, Mesh* m)
 
 void Batch::reset_graph()
 {
-  if (exec_) cudaGraphExecDestroy(exec_);
-  if (graph_) cudaGraphDestroy(graph_);
-  exec_ = nullptr;
-  graph_ = nullptr;
+  for (int k = 0; k < 2; k++) {
+    if (exec_[k]) cudaGraphExecDestroy(exec_[k]);
+    if (graph_[k]) cudaGraphDestroy(graph_[k]);
+    exec_[k] = nullptr;
+    graph_[k] = nullptr;
+  }
+  reserve_ = 0;
 }
 
 int batch_width(int cols) { return cols <= 1 ? 1 : (cols <= 3 ? 3 : 4); }
@@ -100,27 +103,38 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   grid_ = std::min(nsm * occ, std::max(1, nitems_));
+  occ_ = occ;
+  nsm_ = nsm;
   return EB_OK;
 }
 
-int Batch::run(cudaStream_t st)
+int Batch::run(cudaStream_t st, int reserve_sms)
 {
   if (entries_.empty()) return EB_OK;
   const int n = (int)entries_.size();
+  const int free_sms = std::max(1, nsm_ - std::max(0, reserve_sms));
+  const int grid = reserve_sms > 0 ? std::min(grid_, free_sms * occ_) : grid_;
   EB_CUDA(prep_launch_batch(fp32_, nsl_, false, args_.as<ApplyArgs>(), prep_off_.as<int>(), n, prep_blocks_, st));
   EB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(int), st));
   EB_CUDA(far_launch(fp32_, nsl_, false, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
-                     counter_.as<int>(), smem_, grid_, st));
+                     counter_.as<int>(), smem_, grid, st));
   EB_CUDA(finalize_launch_batch(nsl_, false, args_.as<ApplyArgs>(), fin_off_.as<int>(), n, fin_blocks_, st));
   return EB_OK;
 }
 
-int Batch::run_graph(cudaStream_t st)
+int Batch::run_graph(cudaStream_t st, int reserve_sms)
 {
   if (entries_.empty()) return EB_OK;
-  if (!exec_) {
+  const int k = reserve_sms > 0 ? 1 : 0;
+  if (k == 1 && exec_[1] && reserve_sms != reserve_) {  // a different reservation: capture again
+    cudaGraphExecDestroy(exec_[1]);
+    cudaGraphDestroy(graph_[1]);
+    exec_[1] = nullptr;
+    graph_[1] = nullptr;
+  }
+  if (!exec_[k]) {
     EB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int rc = run(st);
+    const int rc = run(st, reserve_sms);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &g);
     if (rc != EB_OK) {
@@ -128,10 +142,11 @@ int Batch::run_graph(cudaStream_t st)
       return rc;
     }
     EB_CUDA(e);
-    graph_ = g;
-    EB_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+    graph_[k] = g;
+    EB_CUDA(cudaGraphInstantiate(&exec_[k], graph_[k], 0));
+    if (k == 1) reserve_ = reserve_sms;
   }
-  EB_CUDA(cudaGraphLaunch(exec_, st));
+  EB_CUDA(cudaGraphLaunch(exec_[k], st));
   return EB_OK;
 }
 

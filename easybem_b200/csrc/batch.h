@@ -37,9 +37,13 @@ class Batch {
   // entry's systems carry zeros).
   int build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags);
   // One apply of all entries whose flag is set (inputs tin, outputs vout).
-  int run(cudaStream_t st);
-  // Captures run() into a CUDA graph on first use and replays it afterwards.
-  int run_graph(cudaStream_t st);
+  // reserve_sms > 0 sizes the persistent far-field grid to leave that many
+  // SMs free for kernels of other streams (the far kernel holds every SM it
+  // starts on until the whole apply is done).
+  int run(cudaStream_t st, int reserve_sms = 0);
+  // Captures run() into a CUDA graph on first use (one graph per grid size)
+  // and replays it afterwards.
+  int run_graph(cudaStream_t st, int reserve_sms = 0);
   void reset_graph();
   ~Batch() { reset_graph(); }
 
@@ -51,11 +55,13 @@ class Batch {
   bool fp32_ = true;
   int nsl_ = kBatchCols;
   DevBuf desc_, items_, args_, prep_off_, fin_off_, counter_;
-  int nitems_ = 0, grid_ = 0, prep_blocks_ = 0, fin_blocks_ = 0, K_ = 0, Q_ = 0;
+  int nitems_ = 0, grid_ = 0, occ_ = 1, nsm_ = 148, prep_blocks_ = 0, fin_blocks_ = 0, K_ = 0, Q_ = 0;
   size_t smem_ = 0;
   long long quad_pairs_ = 0;
-  cudaGraph_t graph_ = nullptr;
-  cudaGraphExec_t exec_ = nullptr;
+  // graphs of the full grid [0] and of the reduced grid [1] (reserve_ SMs left free)
+  cudaGraph_t graph_[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+  int reserve_ = 0;
 };
 
 // Far-field variant width (SL charges) for entries using up to `cols` columns.

@@ -3,6 +3,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -39,11 +40,33 @@ int DevBuf::alloc(size_t n)
   return EB_OK;
 }
 
+int TmpBuf::alloc(size_t n)
+{
+  release();
+  if (n == 0) n = 16;
+  cudaError_t e = cudaMallocAsync(&p, n, st);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    return set_error(e == cudaErrorMemoryAllocation ? EB_ERR_NOMEM : EB_ERR_CUDA,
+                     std::string("cudaMallocAsync(") + std::to_string(n) + "): " + cudaGetErrorString(e));
+  }
+  bytes = n;
+  return EB_OK;
+}
+
 template <typename T>
 static int upload(DevBuf& b, const std::vector<T>& v)
 {
   EB_CHECK(b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1)));
   if (!v.empty()) EB_CUDA(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return EB_OK;
+}
+
+template <typename T>
+static int upload(TmpBuf& b, const std::vector<T>& v)
+{
+  EB_CHECK(b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1)));
+  if (!v.empty()) EB_CUDA(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, b.st));
   return EB_OK;
 }
 
@@ -211,34 +234,42 @@ static int build_near(Mesh* m)
   HostMesh& h = m->h;
   const int npairs = (int)h.sl_col.size();
   m->npairs = npairs;
-  DevBuf d_nodes, d_elems, d_pi, d_pj, d_dle, d_cptr, d_contrib;
-  EB_CHECK(upload(d_nodes, h.nodes));
-  EB_CHECK(upload(d_elems, h.elems));
-  EB_CHECK(upload(d_pi, h.pair_i));
-  EB_CHECK(upload(d_pj, h.sl_col));
   EB_CHECK(upload(m->sl_rowptr, h.sl_rowptr));
   EB_CHECK(upload(m->sl_col, h.sl_col));
   EB_CHECK(upload(m->dl_rowptr, h.dl_rowptr));
   EB_CHECK(upload(m->dl_col, h.dl_col));
-  EB_CHECK(upload(d_cptr, h.dl_contrib_ptr));
-  EB_CHECK(upload(d_contrib, h.dl_contrib));
   EB_CHECK(m->sl_val.alloc(sizeof(double) * std::max(npairs, 1)));
-  EB_CHECK(d_dle.alloc(sizeof(double) * 3 * std::max(npairs, 1)));
   const int nslots = (int)h.dl_col.size();
   EB_CHECK(m->dl_val.alloc(sizeof(double) * std::max(nslots, 1)));
-  // a private stream: mesh set-up overlaps work other threads run on the GPU
+  // a private stream with stream-ordered temporaries: mesh set-up overlaps
+  // work that other threads run on the GPU and never waits for the device
   cudaStream_t st = nullptr;
   EB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  if (npairs > 0)
-    near_values_kernel<<<(npairs + 127) / 128, 128, 0, st>>>(h.quad, d_nodes.as<double>(), d_elems.as<int>(),
-                                                             d_pi.as<int>(), d_pj.as<int>(), npairs,
-                                                             m->sl_val.as<double>(), d_dle.as<double>());
-  if (nslots > 0)
-    dl_gather_kernel<<<(nslots + 255) / 256, 256, 0, st>>>(d_cptr.as<int>(), d_contrib.as<int>(),
-                                                          d_dle.as<double>(), nslots, m->dl_val.as<double>());
-  const cudaError_t e1 = cudaGetLastError();
-  const cudaError_t e2 = cudaStreamSynchronize(st);
+  int rc = EB_OK;
+  cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
+  {
+    TmpBuf d_nodes(st), d_elems(st), d_pi(st), d_pj(st), d_dle(st), d_cptr(st), d_contrib(st);
+    rc = upload(d_nodes, h.nodes);
+    if (rc == EB_OK) rc = upload(d_elems, h.elems);
+    if (rc == EB_OK) rc = upload(d_pi, h.pair_i);
+    if (rc == EB_OK) rc = upload(d_pj, h.sl_col);
+    if (rc == EB_OK) rc = upload(d_cptr, h.dl_contrib_ptr);
+    if (rc == EB_OK) rc = upload(d_contrib, h.dl_contrib);
+    if (rc == EB_OK) rc = d_dle.alloc(sizeof(double) * 3 * std::max(npairs, 1));
+    if (rc == EB_OK) {
+      if (npairs > 0)
+        near_values_kernel<<<(npairs + 127) / 128, 128, 0, st>>>(h.quad, d_nodes.as<double>(), d_elems.as<int>(),
+                                                                 d_pi.as<int>(), d_pj.as<int>(), npairs,
+                                                                 m->sl_val.as<double>(), d_dle.as<double>());
+      if (nslots > 0)
+        dl_gather_kernel<<<(nslots + 255) / 256, 256, 0, st>>>(d_cptr.as<int>(), d_contrib.as<int>(),
+                                                              d_dle.as<double>(), nslots, m->dl_val.as<double>());
+      e1 = cudaGetLastError();
+    }
+  }  // temporaries released on st
+  e2 = cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
+  EB_CHECK(rc);
   EB_CUDA(e1);
   EB_CUDA(e2);
   return EB_OK;
@@ -281,7 +312,8 @@ int mesh_set_plan(Mesh* m, int items_per_sm, int tile)
 {
   if (items_per_sm < 1 || items_per_sm > 4096 || tile < 0 || tile > kTS)
     return set_error(EB_ERR_INVALID, "plan needs 1 <= items_per_sm <= 4096 and 0 <= tile <= " + std::to_string(kTS));
-  EB_CUDA(cudaDeviceSynchronize());
+  // no device-wide synchronisation here: it would break a CUDA graph capture
+  // running in another thread; the caller guarantees no work on m is in flight
   m->plan.items_per_sm = items_per_sm;
   m->plan.tile = tile;
   // per-variant descriptors and the scratch sized for the old split go away
@@ -302,11 +334,20 @@ int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int orde
     return set_error(EB_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
   Mesh* m = new Mesh();
   cudaGetDevice(&m->device);
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
   int st = prepare_host_mesh(nv, nodes, ne, elems1, order, &m->h);
   if (st == EB_OK) tuned_plan_for(m->h, &m->plan.items_per_sm, &m->plan.tile);
+  const auto t1 = clk::now();
   if (st == EB_OK) st = build_static(m);
+  const auto t2 = clk::now();
   if (st == EB_OK) st = build_near(m);
+  const auto t3 = clk::now();
   if (st == EB_OK) st = build_items(m);
+  const auto sec = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+  m->setup_s[0] = sec(t0, t1);
+  m->setup_s[1] = sec(t1, t2);
+  m->setup_s[2] = sec(t2, t3);
   if (st != EB_OK) {
     delete m;
     return st;
@@ -578,7 +619,7 @@ int eb_dirichlet_rhs(eb_mesh mesh, int nrhs, const double* g, double* b)
   // 1/r^3 evaluation); a single set, or the last one of an odd group, uses the
   // one-column variant, groups of two or three are padded with zero columns
   constexpr int kCols = 4;
-  eb::DevBuf du, dq;
+  eb::TmpBuf du(st), dq(st);  // stream-ordered: no device-wide wait when they go
   EB_CHECK(du.alloc(sizeof(double) * kCols * (size_t)h.nv));
   EB_CHECK(dq.alloc(sizeof(double) * kCols * (size_t)h.ne));
   for (int c0 = 0; c0 < nrhs; c0 += kCols) {

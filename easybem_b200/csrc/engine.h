@@ -22,6 +22,30 @@ cudaError_t prep_launch_batch(bool fp32, int NSL, int ND, const ApplyArgs* d_arg
 cudaError_t finalize_launch_batch(int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
                                   cudaStream_t st);
 
+// Temporary device buffer ordered on a stream (cudaMallocAsync /
+// cudaFreeAsync): unlike cudaFree, releasing it does not wait for the whole
+// device, so set-up work on a private stream does not stall behind kernels
+// that other threads keep running. release() must come before the stream is
+// destroyed.
+struct TmpBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  explicit TmpBuf(cudaStream_t s) : st(s) {}
+  TmpBuf(const TmpBuf&) = delete;
+  TmpBuf& operator=(const TmpBuf&) = delete;
+  ~TmpBuf() { release(); }
+  void release()
+  {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    bytes = 0;
+  }
+  int alloc(size_t n);
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
 // Simple owning device buffer.
 struct DevBuf {
   void* p = nullptr;
@@ -81,6 +105,8 @@ struct Mesh {
     int src_tile = 0;
   };
   Variant variants[128];
+  // host seconds of mesh creation: topology and pairs, static tables, near field
+  double setup_s[3] = {0.0, 0.0, 0.0};
   // optional event timing of the far-field kernel
   bool profile = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
@@ -108,7 +134,7 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
 // v = V1 t, P1 x P1 single layer; t and v have nnodes entries (device).
 int mesh_apply_sl_p1(Mesh* m, int precision, const double* d_t, double* d_v, cudaStream_t st);
 // Replaces the launch plan (work split, source tile) of a mesh; later applies
-// and batches use it. Waits for the mesh's work to finish first.
+// and batches use it. No work on the mesh may be in flight.
 int mesh_set_plan(Mesh* m, int items_per_sm, int tile);
 // The tuned plan recorded for meshes like m (returns false if none).
 bool tuned_plan_for(const HostMesh& h, int* items_per_sm, int* tile);

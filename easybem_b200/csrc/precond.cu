@@ -161,19 +161,27 @@ int ensure_near_precond(Mesh* m)
       if (f == e || *f != i) return set_error(EB_ERR_MESH, "near-field pattern is not symmetric");
       tpos[p] = (int)(f - h.sl_col.data());
     }
-  DevBuf d_tpos;
-  EB_CHECK(d_tpos.alloc(sizeof(int) * tpos.size()));
-  EB_CUDA(cudaMemcpy(d_tpos.p, tpos.data(), sizeof(int) * tpos.size(), cudaMemcpyHostToDevice));
   DevBuf pc;
   EB_CHECK(pc.alloc(sizeof(double) * std::max(nnz, 1)));
   cudaStream_t st = nullptr;
   EB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  if (h.ne > 0)
-    near_spai_kernel<<<(h.ne + kPcWarps - 1) / kPcWarps, 32 * kPcWarps, 0, st>>>(
-        h.ne, m->sl_rowptr.as<int>(), m->sl_col.as<int>(), m->sl_val.as<double>(), d_tpos.as<int>(), pc.as<double>());
-  const cudaError_t e1 = cudaGetLastError();
+  int rc = EB_OK;
+  cudaError_t e1 = cudaSuccess;
+  {
+    TmpBuf d_tpos(st);  // stream-ordered: released without a device-wide wait
+    rc = d_tpos.alloc(sizeof(int) * tpos.size());
+    if (rc == EB_OK) {
+      e1 = cudaMemcpyAsync(d_tpos.p, tpos.data(), sizeof(int) * tpos.size(), cudaMemcpyHostToDevice, st);
+      if (e1 == cudaSuccess && h.ne > 0)
+        near_spai_kernel<<<(h.ne + kPcWarps - 1) / kPcWarps, 32 * kPcWarps, 0, st>>>(
+            h.ne, m->sl_rowptr.as<int>(), m->sl_col.as<int>(), m->sl_val.as<double>(), d_tpos.as<int>(),
+            pc.as<double>());
+      if (e1 == cudaSuccess) e1 = cudaGetLastError();
+    }
+  }
   const cudaError_t e2 = cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
+  EB_CHECK(rc);
   EB_CUDA(e1);
   EB_CUDA(e2);
   std::swap(m->pc_val.p, pc.p);

@@ -4,10 +4,11 @@
 // its answer is the Neumann data t solving V t = (1/2 M + K) g for each set.
 // Requests pass through four states:
 //   queued   -> submitted, waiting for device memory;
-//   preparing-> admitted under the memory budget; a host worker thread builds
-//               the mesh (topology, FP64 Sauter-Schwab near field) and the
-//               right-hand sides on the request's own stream, overlapping the
-//               solves already running on the GPU;
+//   preparing-> admitted under the memory budget; one of several host worker
+//               threads builds the mesh (topology, FP64 Sauter-Schwab near
+//               field, preconditioner) and the right-hand sides on the
+//               request's own stream, overlapping the solves already running
+//               on the GPU (which leave a quarter of the SMs free meanwhile);
 //   active   -> its systems joined the shared SolverPool: every step() advances
 //               all active systems by one batched GMRES iteration, so requests
 //               that arrive later join the running batch as soon as they are
@@ -88,7 +89,10 @@ class Server {
   {
     cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
     cudaGetDevice(&device_);
-    worker_ = std::thread([this] { prepare_loop(); });
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
+    reserve_sms_ = nsm / 4;
+    for (int k = 0; k < kPrepWorkers; k++) workers_.emplace_back([this] { prepare_loop(); });
   }
   ~Server()
   {
@@ -97,7 +101,7 @@ class Server {
       stop_ = true;
     }
     cv_.notify_all();
-    worker_.join();
+    for (auto& w : workers_) w.join();
     for (auto& kv : reqs_)
       if (kv.second->mesh) eb_mesh_destroy(kv.second->mesh);
     cudaStreamDestroy(stream_);
@@ -132,10 +136,38 @@ class Server {
 
   int step(int* nactive, int* nwaiting)
   {
+    const double t_enter = now_ms();
+    const int rc = step_impl(nactive, nwaiting);
+    std::lock_guard<std::mutex> g(mu_);
+    n_steps_++;
+    t_step_ms_ += now_ms() - t_enter;
+    return rc;
+  }
+
+  // steps, seconds in step(), batch rebuilds, seconds in them, requests
+  // prepared, seconds the preparation workers were busy, of which mesh
+  // creation, right-hand sides and preconditioner, and mesh creation split
+  // into topology, static tables and near field
+  void stats(double* out, int n)
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    const double v[12] = {(double)n_steps_, 1e-3 * t_step_ms_, (double)pool_.rebuilds(), pool_.rebuild_seconds(),
+                          (double)n_prepared_, 1e-3 * (t_mesh_ms_ + t_rhs_ms_ + t_pc_ms_), 1e-3 * t_mesh_ms_,
+                          1e-3 * t_rhs_ms_, 1e-3 * t_pc_ms_, t_setup_s_[0], t_setup_s_[1], t_setup_s_[2]};
+    for (int k = 0; k < n && k < 12; k++) out[k] = v[k];
+  }
+
+ private:
+  int step_impl(int* nactive, int* nwaiting)
+  {
     cudaSetDevice(device_);
     // join prepared requests (slots permitting)
     {
       std::unique_lock<std::mutex> g(mu_);
+      // while meshes are being prepared, the solver's far field leaves a
+      // quarter of the SMs to the preparation kernels (near field, right-hand
+      // sides, preconditioner), which would otherwise wait for every step
+      pool_.set_reserved_sms(preparing_ > 0 || !to_prepare_.empty() ? reserve_sms_ : 0);
       // nothing to run yet but meshes in preparation: wait (bounded) for the
       // first one instead of returning at once, so callers need not spin
       if (active_.empty() && prepared_.empty() && (preparing_ > 0 || !to_prepare_.empty()))
@@ -203,6 +235,7 @@ class Server {
     return EB_OK;
   }
 
+ public:
   int poll(long long id, int* state)
   {
     std::lock_guard<std::mutex> g(mu_);
@@ -279,16 +312,30 @@ class Server {
         preparing_++;
       }
       eb_mesh m = nullptr;
+      const double t0 = now_ms();
       int rc = eb_mesh_create(r->nv, r->nodes.data(), r->ne, r->elems.data(), r->order, &m);
+      // many meshes share each batched launch: a coarser split per mesh keeps
+      // the merged work list (and the partial sums) small while still giving
+      // every persistent CTA many items
+      if (rc == EB_OK) rc = mesh_set_plan(eb_mesh_internal(m), kServeItemsPerSm, 0);
+      const double t1 = now_ms();
       std::vector<double> b;
       if (rc == EB_OK) {
         b.resize((size_t)r->nrhs * r->ne);
         rc = eb_dirichlet_rhs(m, r->nrhs, r->g.data(), b.data());
       }
+      const double t2 = now_ms();
       if (rc == EB_OK && opt_.precond) rc = ensure_near_precond(eb_mesh_internal(m));
+      const double t3 = now_ms();
       std::string err = rc == EB_OK ? "" : last_error();
       std::lock_guard<std::mutex> g(mu_);
       preparing_--;
+      n_prepared_++;
+      if (m)
+        for (int k = 0; k < 3; k++) t_setup_s_[k] += eb_mesh_internal(m)->setup_s[k];
+      t_mesh_ms_ += t1 - t0;
+      t_rhs_ms_ += t2 - t1;
+      t_pc_ms_ += t3 - t2;
       ready_cv_.notify_all();  // under the lock: step() sees the new state once it wakes
       if (rc != EB_OK) {
         if (m) eb_mesh_destroy(m);
@@ -320,9 +367,14 @@ class Server {
   std::condition_variable cv_;
   std::condition_variable ready_cv_;  // a prepared (or failed) request is ready for step()
   bool stop_ = false;
-  std::thread worker_;
+  static constexpr int kPrepWorkers = 4;      // host threads preparing meshes (topology, near field, RHS)
+  static constexpr int kServeItemsPerSm = 4;  // work split of served meshes (see prepare_loop)
+  std::vector<std::thread> workers_;
+  int reserve_sms_ = 0;
   long long next_id_ = 1;
   int active_systems_ = 0, preparing_ = 0;
+  long long n_steps_ = 0, n_prepared_ = 0;
+  double t_step_ms_ = 0, t_mesh_ms_ = 0, t_rhs_ms_ = 0, t_pc_ms_ = 0, t_setup_s_[3] = {0, 0, 0};
   std::map<long long, std::shared_ptr<Request>> reqs_;
   std::deque<std::shared_ptr<Request>> queue_, to_prepare_, prepared_;
   std::vector<std::shared_ptr<Request>> active_;
@@ -399,6 +451,13 @@ int eb_server_usage(eb_server s, long long* used_bytes, long long* budget_bytes)
 {
   if (!s) return set_error(EB_ERR_INVALID, "null server");
   s->srv->usage(used_bytes, budget_bytes);
+  return EB_OK;
+}
+
+int eb_server_stats(eb_server s, double* stats, int n)
+{
+  if (!s || !stats || n < 0) return set_error(EB_ERR_INVALID, "null argument");
+  s->srv->stats(stats, n);
   return EB_OK;
 }
 

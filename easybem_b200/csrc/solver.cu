@@ -1,6 +1,7 @@
 #include "solver.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -271,7 +272,12 @@ bool SolverPool::done(int id) const
 
 int SolverPool::step(cudaStream_t st, int* nactive)
 {
-  if (dirty_) EB_CHECK(rebuild());
+  if (dirty_) {
+    const auto t0 = std::chrono::steady_clock::now();
+    EB_CHECK(rebuild());
+    n_rebuild_++;
+    t_rebuild_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
   const int S = (int)sys_.size(), m = opt_.restart;
   const int E = (int)entries_.size();
   if (S == 0 || active() == 0) {
@@ -308,14 +314,14 @@ int SolverPool::step(cudaStream_t st, int* nactive)
   if (any_ref) {
     if (any_apply64) {
       k_load<<<eg, 256, 0, st>>>(T, d_phase_.as<int>(), d_k_.as<int>(), kRefine, 0);
-      EB_CHECK(batch_fp64_.run_graph(st));
+      EB_CHECK(batch_fp64_.run_graph(st, reserve_sms_));
     }
     k_residual<<<eg, 256, 0, st>>>(T, d_phase_.as<int>(), d_fresh_.as<int>(), kRefine);
     k_norm<<<S, kRed, 0, st>>>(T, d_phase_.as<int>(), kRefine, 0, d_rn_.as<double>());
   }
   if (any_arn) {
     k_load<<<eg, 256, 0, st>>>(T, d_phase_.as<int>(), d_k_.as<int>(), kArnoldi, 1);
-    EB_CHECK(batch_inner_.run_graph(st));
+    EB_CHECK(batch_inner_.run_graph(st, reserve_sms_));
     const dim3 dg(m + 1, S);
     k_dots<<<dg, kRed, 0, st>>>(T, d_phase_.as<int>(), d_k_.as<int>(), m, kArnoldi, d_h1_.as<double>());
     k_update<<<eg, 256, 0, st>>>(T, d_phase_.as<int>(), d_k_.as<int>(), m, kArnoldi, d_h1_.as<double>());

@@ -56,6 +56,11 @@ class SolverPool {
   int remove(int id);
   size_t device_bytes_per_system(const Mesh* m) const;
   int active() const;
+  // SMs the batched far field leaves free for other streams (0: none).
+  void set_reserved_sms(int n) { reserve_sms_ = n; }
+  // Batch rebuilds after membership changes: count and host seconds spent.
+  long long rebuilds() const { return n_rebuild_; }
+  double rebuild_seconds() const { return t_rebuild_; }
 
  private:
   enum Phase { kRefine = 0, kArnoldi = 1, kDone = 2 };
@@ -91,6 +96,9 @@ class SolverPool {
   DevBuf d_eflag_inner_, d_eflag_fp64_;
   std::vector<double> h1_, h2_, wn_, rn_;
   std::vector<int> phase_, k_, fresh_, fstart_, fx_;
+  int reserve_sms_ = 0;
+  long long n_rebuild_ = 0;
+  double t_rebuild_ = 0.0;
 };
 
 }  // namespace eb

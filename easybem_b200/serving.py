@@ -50,6 +50,7 @@ def run_stream(requests, budget_bytes=120 * 10 ** 9, max_systems=4096, keep_resu
         if active == 0 and waiting == 0 and k < len(pending):
             time.sleep(max(0.0, min(0.01, pending[k]["t_arrival"] - (time.perf_counter() - t0))))
     wall = time.perf_counter() - t0
+    counters = srv.stats()
     srv.close()
     ok = [d for d in done.values() if d.get("stats")]
     lat = [d["times"]["latency_ms"] for d in ok]
@@ -66,5 +67,6 @@ def run_stream(requests, budget_bytes=120 * 10 ** 9, max_systems=4096, keep_resu
         "p99_queue_ms": percentile([d["times"]["queue_ms"] for d in ok], 99),
         "max_rel_residual": max((s["rel_residual"] for d in ok for s in d["stats"]), default=None),
         "iterations_mean": float(np.mean([s["iterations"] for d in ok for s in d["stats"]])) if ok else None,
+        "server": counters,
         "results": done if keep_results else None,
     }

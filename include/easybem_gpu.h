@@ -201,6 +201,13 @@ int eb_server_poll(eb_server server, long long id, int* state);
 int eb_server_result(eb_server server, long long id, double* t, eb_solve_stats* stats, double* times_ms);
 int eb_server_release(eb_server server, long long id);
 int eb_server_usage(eb_server server, long long* used_bytes, long long* budget_bytes);
+/* Operating counters, up to n of: steps, seconds spent in eb_server_step,
+ * solver batch rebuilds (membership changes), seconds spent in them,
+ * requests prepared, seconds the preparation worker was busy, and of those
+ * the seconds in mesh creation, right-hand sides and preconditioner builds,
+ * and mesh creation split into topology, static tables and near field.
+ * No counterpart in the reference. */
+int eb_server_stats(eb_server server, double* stats, int n);
 
 /* Right-hand side of the direct (Green) formulation of the interior Dirichlet
  * problem, as the reference examples build it (python/examples/
@@ -236,9 +243,10 @@ int eb_last_kernel_ms(eb_mesh mesh, double* far_ms, double* finalize_ms);
 /* Launch plan of a mesh's far field: work items per SM (how finely the source
  * range of every 128-target tile is cut for the persistent CTAs' queue) and
  * source triangles per shared-memory tile (0 = the variant's default, at most
- * 64). eb_mesh_set_plan waits for the device, rebuilds the work list and drops
- * the cached launch descriptors; batches and solvers built later use the new
- * plan. Not to be called while another call on the same mesh runs. Results
+ * 64). eb_mesh_set_plan rebuilds the work list and drops the cached launch
+ * descriptors; batches and solvers built later use the new plan. No work on
+ * the mesh may be in flight (synchronise its streams first), and no other
+ * call on the same mesh may run meanwhile. Results
  * change only by rounding (summation order). No counterpart in the reference,
  * whose launch shape is fixed (src/BEM3dLaplaceGPU.cu:985-1322, 256 threads). */
 int eb_mesh_set_plan(eb_mesh mesh, int items_per_sm, int src_tile);
