@@ -376,7 +376,7 @@ class Server:
         return u.value, b.value
 
     STAT_NAMES = ("steps", "step_s", "rebuilds", "rebuild_s", "prepared", "prepare_s", "mesh_s", "rhs_s",
-                  "precond_s", "mesh_topology_s", "mesh_tables_s", "mesh_near_s")
+                  "precond_s", "mesh_topology_s", "mesh_tables_s", "mesh_near_s", "tables_alloc_s", "tables_copy_s")
 
     def stats(self):
         """Operating counters: steps and time in step(), solver batch rebuilds,

@@ -37,6 +37,8 @@ _SIGNATURES = {
     "eb_mesh_info": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "eb_mesh_finalize_bytes": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_release_cached_memory": (ctypes.c_int, []),
+    "eb_cached_memory_bytes": (ctypes.c_int, [ctypes.POINTER(ctypes.c_longlong)]),
     "eb_apply_sl_p0": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_apply_dl_p1": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
     "eb_apply_sl_dl": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp, _dp, _dp]),

@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <iterator>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -25,19 +27,110 @@ int set_error(int status, const std::string& msg)
 
 const char* last_error() { return g_last_error.c_str(); }
 
+// ---------------------------------------------------------------------------
+// Device memory behind DevBuf: the device's stream-ordered pool, kept warm.
+//
+// cudaMalloc and cudaFree, called from a thread that prepares a mesh while
+// other threads keep the GPU busy, were measured to wait for running kernels
+// (cudaFree for the whole device); allocations from a pool that keeps its
+// memory (release threshold at the maximum) return in about 0.1 ms. Every
+// host thread allocates and frees on its own non-blocking stream per device
+// and synchronises after allocating, so a block is usable on any stream at
+// once; it is freed only once no queued work uses it (every caller
+// synchronises first).
+
+namespace {
+
+constexpr int kPoolDevices = 64;
+
+cudaStream_t pool_stream(int dev)
+{
+  struct Streams {
+    cudaStream_t st[kPoolDevices] = {};
+    ~Streams()
+    {
+      for (int d = 0; d < kPoolDevices; d++)
+        if (st[d]) cudaStreamDestroy(st[d]);
+    }
+  };
+  static thread_local Streams s;
+  if (dev < 0 || dev >= kPoolDevices) return nullptr;
+  if (!s.st[dev]) {
+    static std::mutex mu;
+    static bool warm[kPoolDevices] = {};
+    {
+      std::lock_guard<std::mutex> g(mu);
+      if (!warm[dev]) {  // keep freed memory in the pool for later allocations
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+          uint64_t thr = UINT64_MAX;
+          cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        warm[dev] = true;
+      }
+    }
+    if (cudaStreamCreateWithFlags(&s.st[dev], cudaStreamNonBlocking) != cudaSuccess) s.st[dev] = nullptr;
+  }
+  return s.st[dev];
+}
+
+}  // namespace
+
+void DevBuf::release()
+{
+  if (p && owns) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    cudaStream_t st = pool_stream(dev);
+    if (st) cudaFreeAsync(p, st);
+    if (cur != dev) cudaSetDevice(cur);
+  }
+  p = nullptr;
+  bytes = 0;
+  owns = true;
+}
+
 int DevBuf::alloc(size_t n)
 {
   if (n <= bytes && p) return EB_OK;
   release();
   if (n == 0) n = 16;
-  cudaError_t e = cudaMalloc(&p, n);
+  cudaGetDevice(&dev);
+  cudaStream_t st = pool_stream(dev);
+  if (!st) return set_error(EB_ERR_CUDA, "cannot create an allocation stream");
+  cudaError_t e = cudaMallocAsync(&p, n, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     p = nullptr;
     return set_error(e == cudaErrorMemoryAllocation ? EB_ERR_NOMEM : EB_ERR_CUDA,
-                     std::string("cudaMalloc(") + std::to_string(n) + "): " + cudaGetErrorString(e));
+                     std::string("cudaMallocAsync(") + std::to_string(n) + "): " + cudaGetErrorString(e));
   }
   bytes = n;
   return EB_OK;
+}
+
+int devmem_trim(int device)
+{
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return EB_OK;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(device);
+  cudaDeviceSynchronize();
+  cudaMemPoolTrimTo(pool, 0);
+  cudaSetDevice(cur);
+  return EB_OK;
+}
+
+size_t devmem_cached_bytes(int device)
+{
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return 0;
+  uint64_t reserved = 0, used = 0;
+  cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+  cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  return reserved > used ? (size_t)(reserved - used) : 0;
 }
 
 int TmpBuf::alloc(size_t n)
@@ -206,26 +299,45 @@ static int build_static(Mesh* m)
       }
     ttile[t] = dq{c.x, c.y, c.z, std::sqrt(r2) * (1.0 + 1e-12)};
   }
-  EB_CHECK(upload(m->pos32, pos32));
-  EB_CHECK(upload(m->pos64, pos64));
-  EB_CHECK(upload(m->wj, wjtab));
-  EB_CHECK(upload(m->trin, trin));
-  EB_CHECK(upload(m->svid, svid));
-  EB_CHECK(upload(m->perm, h.perm));
-  EB_CHECK(upload(m->iperm, h.iperm));
-  EB_CHECK(upload(m->bary, bary));
-  EB_CHECK(upload(m->tgt32, tgt32));
-  EB_CHECK(upload(m->tgt64, tgt64));
-  EB_CHECK(upload(m->tgtw32, tgtw32));
-  EB_CHECK(upload(m->tgtw64, tgtw64));
-  EB_CHECK(upload(m->tcent, tcent));
-  EB_CHECK(upload(m->tnrm, tnrm));
-  EB_CHECK(upload(m->snrm, snrm));
-  EB_CHECK(upload(m->tvid, tvid));
-  EB_CHECK(upload(m->ccent, ccent));
-  EB_CHECK(upload(m->ttile, ttile));
-  EB_CHECK(upload(m->splane32, splane32));
-  EB_CHECK(upload(m->splane64, splane64));
+  // one allocation and one copy for all static tables (a mesh set-up that
+  // runs beside other GPU work pays the per-call latency of the runtime once)
+  struct Part {
+    DevBuf* dst;
+    const void* src;
+    size_t bytes;
+  };
+  auto part = [](DevBuf& d, const auto& v) {
+    return Part{&d, (const void*)v.data(), sizeof(v[0]) * v.size()};
+  };
+  const Part parts[] = {part(m->pos32, pos32),   part(m->pos64, pos64),     part(m->wj, wjtab),
+                        part(m->trin, trin),     part(m->svid, svid),       part(m->perm, h.perm),
+                        part(m->iperm, h.iperm), part(m->bary, bary),       part(m->tgt32, tgt32),
+                        part(m->tgt64, tgt64),   part(m->tgtw32, tgtw32),   part(m->tgtw64, tgtw64),
+                        part(m->tcent, tcent),   part(m->tnrm, tnrm),       part(m->snrm, snrm),
+                        part(m->tvid, tvid),     part(m->ccent, ccent),     part(m->ttile, ttile),
+                        part(m->splane32, splane32), part(m->splane64, splane64)};
+  auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  size_t total = 0;
+  for (const Part& q : parts) total += align(std::max<size_t>(q.bytes, 16));
+  std::vector<unsigned char> staging(total, 0);
+  size_t off = 0;
+  for (const Part& q : parts) {
+    if (q.bytes) std::memcpy(staging.data() + off, q.src, q.bytes);
+    off += align(std::max<size_t>(q.bytes, 16));
+  }
+  const auto ta = std::chrono::steady_clock::now();
+  EB_CHECK(m->arena.alloc(total));
+  const auto tb = std::chrono::steady_clock::now();
+  EB_CUDA(cudaMemcpy(m->arena.p, staging.data(), total, cudaMemcpyHostToDevice));
+  const auto tc = std::chrono::steady_clock::now();
+  m->setup_s[3] = std::chrono::duration<double>(tb - ta).count();
+  m->setup_s[4] = std::chrono::duration<double>(tc - tb).count();
+  off = 0;
+  for (const Part& q : parts) {
+    const size_t n = align(std::max<size_t>(q.bytes, 16));
+    q.dst->view(static_cast<unsigned char*>(m->arena.p) + off, std::max<size_t>(q.bytes, 16));
+    off += n;
+  }
   return EB_OK;
 }
 
@@ -534,6 +646,23 @@ int eb_mesh_info(eb_mesh mesh, int* nnodes, int* nelems, long long* near_pairs, 
   if (nelems) *nelems = mesh->m->h.ne;
   if (near_pairs) *near_pairs = mesh->m->npairs;
   if (far_quad_pairs) *far_quad_pairs = mesh->m->h.far_quad_pairs;
+  return EB_OK;
+}
+
+int eb_release_cached_memory(void)
+{
+  int n = 0;
+  EB_CUDA(cudaGetDeviceCount(&n));
+  for (int d = 0; d < n; d++) eb::devmem_trim(d);
+  return EB_OK;
+}
+
+int eb_cached_memory_bytes(long long* bytes)
+{
+  if (!bytes) return set_error(EB_ERR_INVALID, "null argument");
+  int dev = 0;
+  EB_CUDA(cudaGetDevice(&dev));
+  *bytes = (long long)eb::devmem_cached_bytes(dev);
   return EB_OK;
 }
 

@@ -22,6 +22,11 @@ cudaError_t prep_launch_batch(bool fp32, int NSL, int ND, const ApplyArgs* d_arg
 cudaError_t finalize_launch_batch(int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
                                   cudaStream_t st);
 
+// Returns the pool memory of a device that no buffer uses to the driver
+// (waits for the device); the bytes the pool holds unused.
+int devmem_trim(int device);
+size_t devmem_cached_bytes(int device);
+
 // Temporary device buffer ordered on a stream (cudaMallocAsync /
 // cudaFreeAsync): unlike cudaFree, releasing it does not wait for the whole
 // device, so set-up work on a private stream does not stall behind kernels
@@ -47,15 +52,26 @@ struct TmpBuf {
 };
 
 // Simple owning device buffer.
+// Owning device buffer from the device's stream-ordered memory pool, which
+// keeps freed memory for reuse (cudaFree waits for the whole device, so
+// releasing a mesh or a solver system while other threads keep the GPU busy
+// would stall them). Memory goes back to the driver only through
+// devmem_trim(). Releasing a buffer is only allowed once no queued work uses
+// it (every caller synchronises first).
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  int dev = 0;
+  bool owns = true;  // false: a view into another buffer (not freed here)
   ~DevBuf() { release(); }
-  void release()
+  void release();
+  // A view of [base, base + n) of a buffer that outlives it.
+  void view(void* base, size_t n)
   {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
+    release();
+    p = base;
+    bytes = n;
+    owns = false;
   }
   int alloc(size_t n);  // no-op when already at least n bytes
   template <typename T>
@@ -76,7 +92,8 @@ struct Mesh {
   HostMesh h;
   int device = 0;
 
-  // static geometry (sorted order)
+  // static geometry (sorted order), views into one allocation (arena)
+  DevBuf arena;
   DevBuf pos32, pos64, wj, trin, svid, perm, iperm, bary;
   DevBuf tgt32, tgt64, tgtw32, tgtw64, tcent, tnrm, tvid, ccent, snrm, ttile, splane32, splane64;
   // P1 x P1 single layer near field (built on first use)
@@ -105,8 +122,9 @@ struct Mesh {
     int src_tile = 0;
   };
   Variant variants[128];
-  // host seconds of mesh creation: topology and pairs, static tables, near field
-  double setup_s[3] = {0.0, 0.0, 0.0};
+  // host seconds of mesh creation: topology and pairs, static tables, near
+  // field, and within the tables their device allocation and copy
+  double setup_s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   // optional event timing of the far-field kernel
   bool profile = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;

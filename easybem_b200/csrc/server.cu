@@ -46,9 +46,8 @@ static double now_ms()
 static size_t mesh_resident_bytes(const Mesh* m)
 {
   size_t b = 0;
-  const DevBuf* bufs[] = {&m->pos32, &m->pos64, &m->wj, &m->trin, &m->svid, &m->perm, &m->iperm, &m->bary,
-                          &m->tgt32, &m->tgt64, &m->tcent, &m->tnrm, &m->tvid, &m->ccent, &m->snrm, &m->ttile,
-                          &m->splane32, &m->splane64, &m->sl_rowptr, &m->sl_col, &m->sl_val, &m->dl_rowptr,
+  // the static tables are views into the arena, which is counted once
+  const DevBuf* bufs[] = {&m->arena, &m->sl_rowptr, &m->sl_col, &m->sl_val, &m->dl_rowptr,
                           &m->dl_col, &m->dl_val, &m->rec, &m->partial, &m->counter, &m->items, &m->io_t,
                           &m->io_u, &m->io_v, &m->io_q, &m->pc_val};
   for (const DevBuf* d : bufs) b += d->bytes;
@@ -146,15 +145,16 @@ class Server {
 
   // steps, seconds in step(), batch rebuilds, seconds in them, requests
   // prepared, seconds the preparation workers were busy, of which mesh
-  // creation, right-hand sides and preconditioner, and mesh creation split
-  // into topology, static tables and near field
+  // creation, right-hand sides and preconditioner, mesh creation split into
+  // topology, static tables and near field, and the tables' allocation and copy
   void stats(double* out, int n)
   {
     std::lock_guard<std::mutex> g(mu_);
-    const double v[12] = {(double)n_steps_, 1e-3 * t_step_ms_, (double)pool_.rebuilds(), pool_.rebuild_seconds(),
+    const double v[14] = {(double)n_steps_, 1e-3 * t_step_ms_, (double)pool_.rebuilds(), pool_.rebuild_seconds(),
                           (double)n_prepared_, 1e-3 * (t_mesh_ms_ + t_rhs_ms_ + t_pc_ms_), 1e-3 * t_mesh_ms_,
-                          1e-3 * t_rhs_ms_, 1e-3 * t_pc_ms_, t_setup_s_[0], t_setup_s_[1], t_setup_s_[2]};
-    for (int k = 0; k < n && k < 12; k++) out[k] = v[k];
+                          1e-3 * t_rhs_ms_, 1e-3 * t_pc_ms_, t_setup_s_[0], t_setup_s_[1], t_setup_s_[2],
+                          t_setup_s_[3], t_setup_s_[4]};
+    for (int k = 0; k < n && k < 14; k++) out[k] = v[k];
   }
 
  private:
@@ -332,7 +332,7 @@ class Server {
       preparing_--;
       n_prepared_++;
       if (m)
-        for (int k = 0; k < 3; k++) t_setup_s_[k] += eb_mesh_internal(m)->setup_s[k];
+        for (int k = 0; k < 5; k++) t_setup_s_[k] += eb_mesh_internal(m)->setup_s[k];
       t_mesh_ms_ += t1 - t0;
       t_rhs_ms_ += t2 - t1;
       t_pc_ms_ += t3 - t2;
@@ -374,7 +374,7 @@ class Server {
   long long next_id_ = 1;
   int active_systems_ = 0, preparing_ = 0;
   long long n_steps_ = 0, n_prepared_ = 0;
-  double t_step_ms_ = 0, t_mesh_ms_ = 0, t_rhs_ms_ = 0, t_pc_ms_ = 0, t_setup_s_[3] = {0, 0, 0};
+  double t_step_ms_ = 0, t_mesh_ms_ = 0, t_rhs_ms_ = 0, t_pc_ms_ = 0, t_setup_s_[5] = {0, 0, 0, 0, 0};
   std::map<long long, std::shared_ptr<Request>> reqs_;
   std::deque<std::shared_ptr<Request>> queue_, to_prepare_, prepared_;
   std::vector<std::shared_ptr<Request>> active_;

@@ -43,12 +43,23 @@ const char* eb_last_error(void);
  * (src/BEM3dLaplaceGPU.cu:830-921 with src/meshTopology.cpp:196-261). */
 int eb_mesh_create(int nnodes, const double* nodes, int nelems, const int* elems, int order,
                    eb_mesh* out);
-/* Releases a mesh. Replaces closeGPU (src/BEM3dLaplaceGPU.cu:924-957). */
+/* Releases a mesh. Replaces closeGPU (src/BEM3dLaplaceGPU.cu:924-957).
+ * Work queued on caller streams with this mesh (the _device applies) must
+ * have completed: its memory goes back to the memory pool at once. */
 int eb_mesh_destroy(eb_mesh mesh);
 /* Sizes: vertices, triangles, near pairs (incl. coincident) and the number of
  * regular quadrature-point pairs one far-field apply evaluates. */
 int eb_mesh_info(eb_mesh mesh, int* nnodes, int* nelems, long long* near_pairs,
                  long long* far_quad_pairs);
+/* The library allocates from each device's stream-ordered memory pool and
+ * keeps freed memory there for reuse (cudaMalloc and cudaFree from a thread
+ * preparing meshes were measured to wait for kernels other threads run).
+ * eb_release_cached_memory returns the unused pool memory to the driver (it
+ * waits for the devices); eb_cached_memory_bytes reports the unused pool
+ * memory of the current device. No counterpart in the reference. */
+int eb_release_cached_memory(void);
+int eb_cached_memory_bytes(long long* bytes);
+
 /* Algorithmic bytes one SL+DL finalize launch moves (near-field CSR, the
  * gathered densities, the far-field partial sums under the current plan and
  * the outputs): the numerator of its HBM roofline. No counterpart in the
@@ -205,7 +216,8 @@ int eb_server_usage(eb_server server, long long* used_bytes, long long* budget_b
  * solver batch rebuilds (membership changes), seconds spent in them,
  * requests prepared, seconds the preparation worker was busy, and of those
  * the seconds in mesh creation, right-hand sides and preconditioner builds,
- * and mesh creation split into topology, static tables and near field.
+ * mesh creation split into topology, static tables and near field, and the
+ * static tables' device allocation and copy.
  * No counterpart in the reference. */
 int eb_server_stats(eb_server server, double* stats, int n);
 
