@@ -9,7 +9,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libeasybem_gpu.so")
+# EASYBEM_B200_LIB may name another build of the library (e.g. for A/B timing)
+LIB_PATH = os.environ.get("EASYBEM_B200_LIB") or os.path.join(HERE, "libeasybem_gpu.so")
 
 EB_OK = 0
 EB_ERR_INVALID = 1

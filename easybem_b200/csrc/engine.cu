@@ -99,6 +99,20 @@ int DevBuf::alloc(size_t n)
   cudaGetDevice(&dev);
   cudaStream_t st = pool_stream(dev);
   if (!st) return set_error(EB_ERR_CUDA, "cannot create an allocation stream");
+  // the pool grows in steps of at least 1 GiB: each growth costs about as much
+  // as a large cudaMalloc, so many small requests should not each pay one
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t reserved = 0, used = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    if (reserved - used < n + (n >> 3)) {
+      void* grow = nullptr;
+      const size_t step = std::max<size_t>(n + (n >> 3), size_t(1) << 30);
+      if (cudaMallocAsync(&grow, step, st) == cudaSuccess) cudaFreeAsync(grow, st);
+      else cudaGetLastError();  // no room for the step: allocate just n below
+    }
+  }
   cudaError_t e = cudaMallocAsync(&p, n, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
