@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -91,7 +92,9 @@ class Server {
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device_);
     reserve_sms_ = nsm / 4;
-    for (int k = 0; k < kPrepWorkers; k++) workers_.emplace_back([this] { prepare_loop(); });
+    int nworkers = kPrepWorkers;
+    if (const char* e = std::getenv("EASYBEM_PREP_WORKERS")) nworkers = std::max(1, std::min(64, std::atoi(e)));
+    for (int k = 0; k < nworkers; k++) workers_.emplace_back([this] { prepare_loop(); });
   }
   ~Server()
   {
@@ -367,7 +370,8 @@ class Server {
   std::condition_variable cv_;
   std::condition_variable ready_cv_;  // a prepared (or failed) request is ready for step()
   bool stop_ = false;
-  static constexpr int kPrepWorkers = 4;      // host threads preparing meshes (topology, near field, RHS)
+  static constexpr int kPrepWorkers = 4;      // host threads preparing meshes (EASYBEM_PREP_WORKERS overrides;
+                                              // 4, 8 and 16 served the same 4.0-4.2 requests/s: the GPU is the limit)
   static constexpr int kServeItemsPerSm = 4;  // work split of served meshes (see prepare_loop)
   std::vector<std::thread> workers_;
   int reserve_sms_ = 0;
