@@ -353,16 +353,21 @@ def run_small(args):
     torch.cuda.set_device(local)
     nodes, elems = meshes.icosphere(3)
     g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
-    t0 = time.perf_counter()
-    m = eb.Mesh(nodes, elems)
-    b = m.dirichlet_rhs(g)
-    [(x, st)] = eb.solve([(m, b)], tol=1e-8)
-    t_gpu = time.perf_counter() - t0
+    def once():
+        t0 = time.perf_counter()
+        m = eb.Mesh(nodes, elems)
+        b = m.dirichlet_rhs(g)
+        [(x, st)] = eb.solve([(m, b)], tol=1e-8)
+        return time.perf_counter() - t0, m, x, st
+
+    t_cold, m, x, st = once()  # includes the process's first kernel loads and memory-pool set-up
+    m.close()
+    t_gpu, m, x, st = once()
     rel = lambda a, c: float(np.linalg.norm(a - c) / np.linalg.norm(c))
     line = {"metric": METRIC, "workload": "small", "value": 1e3 * t_gpu, "unit": "ms (mesh + RHS + solve)",
             "higher_is_better": False, "data": "synthetic",
             "config": {"workload": "unit icosphere L3 (1,280 triangles), Dirichlet g = 1/|x-(0,0,3)|"},
-            "solve": st[0]}
+            "cold_ms": 1e3 * t_cold, "solve": st[0]}
     rng = np.random.default_rng(0)
     dens = rng.normal(size=elems.shape[0])
     if O.ref_available():
