@@ -22,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libeasybem_ref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libeasybem_ref_gpu.so")
 TABLES_NPZ = os.path.join(os.path.dirname(HERE), "tests", "golden", "reference_quadrature.npz")
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -229,6 +230,39 @@ def ref_apply_rows(nodes, elems, t, u, rows=None, nthreads: int = 0, order: int 
                        _d(np.ascontiguousarray(u, dtype=np.float64)), len(rows), _i(rows), _d(v), _d(q),
                        nthreads)
     return v, q
+
+
+def refgpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+def refgpu_apply(nodes, elems, t, u, order: int = 4, repeats: int = 1):
+    """The reference's own GPU path (initGPU, applyGPULaplace3d1Layer/2Layer,
+    src/BEM3dLaplaceGPU.cu:830-1551, FP32 kernels with host-packed pairs),
+    built by `make -C oracle refgpu`. Returns (V t, K u, seconds of the
+    fastest SL apply, seconds of the fastest DL apply, seconds of initGPU)."""
+    import time
+    lib = ctypes.CDLL(REF_GPU_SO)
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    elems = np.ascontiguousarray(elems, dtype=np.int32)
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    v = np.zeros(elems.shape[0])
+    q = np.zeros(elems.shape[0])
+    with _quiet_stdout():
+        a = time.perf_counter()
+        lib.refgpu_init(nodes.shape[0], _d(nodes), elems.shape[0], _i(elems), order)
+        t_init = time.perf_counter() - a
+        t_sl = t_dl = float("inf")
+        for _ in range(repeats):
+            a = time.perf_counter()
+            lib.refgpu_apply_sl(_d(t), _d(v))
+            t_sl = min(t_sl, time.perf_counter() - a)
+            a = time.perf_counter()
+            lib.refgpu_apply_dl(_d(u), _d(q))
+            t_dl = min(t_dl, time.perf_counter() - a)
+        lib.refgpu_close()
+    return v, q, t_sl, t_dl, t_init
 
 
 class _quiet_stdout:
