@@ -20,6 +20,9 @@
 #ifndef EB_UNROLL_B_F64
 #define EB_UNROLL_B_F64 0  // FP64 variants with at most two outputs; wider ones keep a rolled loop
 #endif
+#ifndef EB_UNROLL_WIDE_F64
+#define EB_UNROLL_WIDE_F64 1  // FP64 variants with three or more outputs
+#endif
 #ifndef EB_UNROLL_B_X2
 #define EB_UNROLL_B_X2 0  // source-point unroll of the packed FP32 form (0: full)
 #endif
@@ -108,7 +111,7 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
   constexpr int NREC = rec_slots(NSL, ND);
   // the fully unrolled FP64 loop measured 5 % faster at L6 for SL+DL; with
   // three or more outputs its registers spill, so those variants stay rolled
-  constexpr int kUnroll = std::is_same<T, float>::value ? kUnrollF32 : (NSL + ND <= 2 ? kUnrollF64 : 1);
+  constexpr int kUnroll = std::is_same<T, float>::value ? kUnrollF32 : (NSL + ND <= 2 ? kUnrollF64 : EB_UNROLL_WIDE_F64);
   const int nqr = NQ > 0 ? NQ : nq;
 #pragma unroll 1
   for (int s = s0; s < s1; ++s) {
