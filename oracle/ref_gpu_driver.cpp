@@ -1,8 +1,8 @@
 // C wrappers over the reference's own GPU path (include/BEM3dLaplaceGPU.h:8-18,
 // src/BEM3dLaplaceGPU.cu:830-1555), compiled from the reference sources where
-// they lie by `make -C oracle refgpu`. Test and measurement infrastructure only:
-// bench.py times it as a secondary baseline beside the CPU reference; the
-// product never loads it. Linked with -Bsymbolic so the reference's C++ entry
+// they lie by `make -C oracle refgpu`. Test infrastructure only:
+// tests/test_gpu_vs_reference_gpu.py compares it with this library's applies
+// (results and time) on the same mesh; the product never loads it. Linked with -Bsymbolic so the reference's C++ entry
 // points and globals (same names as this project's legacy shim) bind inside
 // this library.
 #include "BEM3dLaplaceGPU.h"
