@@ -31,6 +31,32 @@ from oracle import oracle as O  # noqa: E402
 REF_CUBE = "/root/reference/python/examples/cube01-surface.txt"
 
 
+def compact(nodes, elems1):
+    """Drops unreferenced vertices and renumbers (1-based elements)."""
+    used = np.unique(elems1 - 1)
+    new = np.full(nodes.shape[0], -1, dtype=np.int64)
+    new[used] = np.arange(used.size)
+    return nodes[used].copy(), (new[elems1 - 1] + 1).astype(np.int32)
+
+
+def open_cap():
+    """An open surface: the perturbed level-2 icosphere without the triangles
+    whose centroid lies above z = 0.6 (a shell with a hole, so some edges
+    belong to one triangle only)."""
+    v, f = meshes.perturbed_icosphere(2, seed=5)
+    cz = v[f - 1][:, :, 2].mean(axis=1)
+    return compact(v, f[cz < 0.6])
+
+
+def two_spheres():
+    """Two disjoint components: a level-1 icosphere and a scaled, rotated and
+    shifted copy of it (pairs across the components are all regular)."""
+    v, f = meshes.icosphere(1)
+    rot = meshes.random_rotation(np.random.default_rng(11))
+    w = (v @ rot.T) * np.array([1.3, 0.8, 1.0]) + np.array([2.5, 0.4, -0.3])
+    return np.vstack([v, w]), np.vstack([f, f + v.shape[0]]).astype(np.int32)
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libeasybem_ref.so is missing: run `make -C oracle ref` first")
@@ -57,6 +83,8 @@ def main():
     cases["pico2"] = (v, f, [0, 1, 2, 3, 4, 5, 6, 8])
     v, f = meshes.torus(16, 0.3)
     cases["torus16"] = (v, f, [4])
+    cases["cap"] = (*open_cap(), [4])
+    cases["pair"] = (*two_spheres(), [4])
     out = {}
     for name, (nodes, elems, orders) in cases.items():
         rng = np.random.default_rng(7)

@@ -19,7 +19,7 @@ FP64_TOL = 1e-12
 MIXED_TOL = 1e-6
 
 
-@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16"])
+@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16", "cap", "pair"])
 def test_small_meshes_match_reference_golden(gpu_lib, golden_ops, name):
     z = golden_ops
     nodes, elems, t, u = z[f"{name}_nodes"], z[f"{name}_elems"], z[f"{name}_t"], z[f"{name}_u"]
@@ -137,7 +137,7 @@ def test_invalid_meshes_are_rejected(gpu_lib):
     assert e.value.status == 1
 
 
-@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16"])
+@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16", "cap", "pair"])
 def test_hypersingular_matches_reference_golden(gpu_lib, golden_ops, name):
     # D u with D assembled by the reference's getLaplace3d (curl form)
     z = golden_ops
@@ -188,7 +188,7 @@ def test_batched_apply_equals_per_mesh_applies(gpu_lib):
         m.close()
 
 
-@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16"])
+@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16", "cap", "pair"])
 def test_potential_evaluation_matches_reference_golden(gpu_lib, golden_ops, name):
     # evaluateLaplace3d of the reference at points inside, outside and near the surface
     z = golden_ops

@@ -13,7 +13,7 @@ from easybem_b200 import meshes
 from oracle import oracle as O
 
 
-@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16"])
+@pytest.mark.parametrize("name", ["cube", "ico2", "pico2", "torus16", "cap", "pair"])
 def test_oracle_matches_golden_default_order(golden_ops, oracle, name):
     z = golden_ops
     nodes, elems, t, u = z[f"{name}_nodes"], z[f"{name}_elems"], z[f"{name}_t"], z[f"{name}_u"]
