@@ -72,6 +72,8 @@ def parse_args(argv=None):
     p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
     p.add_argument("--serve-sample", type=int, default=32,
                    help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
+    p.add_argument("--rhs-precision", default="fp64", choices=["mixed", "fp64"],
+                   help="serve: precision of the served right-hand sides (1/2 M + K) g")
     return p.parse_args(argv)
 
 
@@ -235,14 +237,14 @@ def run_serve(args):
     torch.cuda.set_device(local)
     from easybem_b200.serving import run_stream
     reqs = serve_stream(args.requests, seed=rank)
-    res = run_stream(reqs, budget_bytes=120 * 10 ** 9, tol=1e-8)
+    res = run_stream(reqs, budget_bytes=120 * 10 ** 9, tol=1e-8, rhs_precision=args.rhs_precision)
     res.pop("results", None)
     if rank == 0:
         line = {"metric": METRIC, "workload": "serve", "value": res["p99_ms"], "unit": "ms (p99 request latency)",
                 "higher_is_better": False, "n_gpus": world, "data": "synthetic",
                 "config": {"workload": "2,000 torus Dirichlet solves (512-32,768 triangles, 1-8 RHS), Poisson "
                                        "arrivals at 200/s, 120 GB admission budget, tol 1e-8",
-                           "requests": args.requests},
+                           "requests": args.requests, "rhs_precision": args.rhs_precision},
                 **{k: v for k, v in res.items()}}
         print(json.dumps(line), flush=True)
 
@@ -519,7 +521,8 @@ def main():
     serve = None
     if args.serve_sample > 0 and world == 1:
         from easybem_b200.serving import run_stream
-        serve = run_stream(serve_stream(args.serve_sample), budget_bytes=120 * 10 ** 9, tol=1e-8)
+        serve = run_stream(serve_stream(args.serve_sample), budget_bytes=120 * 10 ** 9, tol=1e-8,
+                           rhs_precision=args.rhs_precision)
         serve.pop("results", None)
     line = {
         "metric": METRIC, "value": value, "unit": "Gpairs/s", "n_gpus": world, "steps": args.steps,
@@ -556,7 +559,7 @@ def main():
     if serve is not None:
         line["serve_sample"] = {"requests": serve["requests"], "p50_ms": serve["p50_ms"], "p99_ms": serve["p99_ms"],
                                 "solves_per_s": serve["solves_per_s"], "converged": serve["converged"],
-                                "max_rel_residual": serve["max_rel_residual"],
+                                "max_rel_residual": serve["max_rel_residual"], "rhs_precision": args.rhs_precision,
                                 "note": "first requests of the 2,000-request Poisson stream (200/s); "
                                         "full stream: bench.py --workload serve"}
     print(json.dumps(line), flush=True)

@@ -146,13 +146,14 @@ class Mesh:
                                           _ptr(u), _ptr(out)))
         return out
 
-    def dirichlet_rhs(self, g):
-        """b = (1/2) M g + K g for vertex data g ([nnodes] or [nrhs, nnodes]), FP64."""
+    def dirichlet_rhs(self, g, precision: str = "fp64"):
+        """b = (1/2) M g + K g for vertex data g ([nnodes] or [nrhs, nnodes]);
+        K g in FP64 (default) or mixed precision (FP32 far field)."""
         g = np.ascontiguousarray(g, dtype=np.float64)
         one = g.ndim == 1
         g2 = g.reshape(-1, self.nnodes)
         b = np.empty((g2.shape[0], self.nelems))
-        check(lib().eb_dirichlet_rhs(self._h, g2.shape[0], _ptr(g2), _ptr(b)))
+        check(lib().eb_dirichlet_rhs_prec(self._h, precision_code(precision), g2.shape[0], _ptr(g2), _ptr(b)))
         return b[0] if one else b
 
     def apply_near_precond(self, x):
@@ -253,7 +254,7 @@ class Solver:
     def __init__(self, tol=1e-8, inner_tol=1e-6, restart=50, max_cycles=40, max_iterations=4000,
                  inner_precision="mixed", precond=True):
         o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision),
-                         1 if precond else 0)
+                         1 if precond else 0, precision_code("fp64"))
         h = ctypes.c_void_p()
         check(lib().eb_solver_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h
@@ -311,15 +312,18 @@ class Server:
     ``submit(nodes, elems, g)`` queues a request (g: [nrhs, nnodes] Dirichlet
     vertex data) and returns its id; ``step()`` advances every running
     request by one iteration; ``result(id)`` returns (t, stats, times) once
-    ``state(id) == 4``.
+    ``state(id) == 4``. ``rhs_precision`` is the precision of the right-hand
+    sides (1/2 M + K) g the server computes: "fp64" (default) or "mixed" (FP32
+    far field of K g; 1/2 M g and K g cancel for data harmonic inside the
+    surface, so b and the solution then carry errors of a few 1e-6).
     """
 
     STATES = {0: "queued", 1: "preparing", 2: "prepared", 3: "solving", 4: "done", 5: "failed"}
 
     def __init__(self, budget_bytes: int, max_systems: int = 4096, tol=1e-8, inner_tol=1e-6, restart=50,
-                 max_cycles=40, max_iterations=4000, inner_precision="mixed", precond=True):
+                 max_cycles=40, max_iterations=4000, inner_precision="mixed", precond=True, rhs_precision="fp64"):
         o = SolveOptions(tol, inner_tol, restart, max_cycles, max_iterations, precision_code(inner_precision),
-                         1 if precond else 0)
+                         1 if precond else 0, precision_code(rhs_precision))
         h = ctypes.c_void_p()
         check(lib().eb_server_create(int(budget_bytes), int(max_systems), ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -55,6 +55,7 @@ _SIGNATURES = {
     "eb_measure_rsqrt_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "eb_set_profiling": (ctypes.c_int, [_dp, ctypes.c_int]),
     "eb_dirichlet_rhs": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
+    "eb_dirichlet_rhs_prec": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, _dp, _dp]),
     "eb_evaluate_potential": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp]),
     "eb_solve_options_default": (None, [_dp]),
     "eb_apply_near_precond": (ctypes.c_int, [_dp, _dp, _dp]),
@@ -97,7 +98,7 @@ _SIGNATURES = {
 class SolveOptions(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("inner_tol", ctypes.c_double), ("restart", ctypes.c_int),
                 ("max_cycles", ctypes.c_int), ("max_iterations", ctypes.c_int), ("inner_precision", ctypes.c_int),
-                ("precond", ctypes.c_int)]
+                ("precond", ctypes.c_int), ("rhs_precision", ctypes.c_int)]
 
 
 class SolveStats(ctypes.Structure):

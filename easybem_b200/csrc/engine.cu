@@ -752,14 +752,21 @@ int eb_apply_sl_dl(eb_mesh mesh, int precision, const double* t, const double* u
 
 int eb_dirichlet_rhs(eb_mesh mesh, int nrhs, const double* g, double* b)
 {
+  return eb_dirichlet_rhs_prec(mesh, EB_PREC_FP64, nrhs, g, b);
+}
+
+int eb_dirichlet_rhs_prec(eb_mesh mesh, int precision, int nrhs, const double* g, double* b)
+{
   if (!mesh || !g || !b || nrhs < 1) return set_error(EB_ERR_INVALID, "null argument");
+  if (precision != EB_PREC_FP64 && precision != EB_PREC_MIXED)
+    return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
   std::lock_guard<std::mutex> lk(mesh->lock);
   eb::Mesh* m = mesh->m;
   EB_CUDA(cudaSetDevice(m->device));
   const eb::HostMesh& h = m->h;
   cudaStream_t st = mesh->stream;
-  // K g in FP64, four data sets per pass (they share every distance and
-  // 1/r^3 evaluation); a single set, or the last one of an odd group, uses the
+  // K g four data sets per pass (they share every distance and 1/r^3
+  // evaluation); a single set, or the last one of an odd group, uses the
   // one-column variant, groups of two or three are padded with zero columns
   constexpr int kCols = 4;
   eb::TmpBuf du(st), dq(st);  // stream-ordered: no device-wide wait when they go
@@ -771,7 +778,7 @@ int eb_dirichlet_rhs(eb_mesh mesh, int nrhs, const double* g, double* b)
     if (nc < nd) EB_CUDA(cudaMemsetAsync(du.p, 0, sizeof(double) * nd * (size_t)h.nv, st));
     EB_CUDA(cudaMemcpyAsync(du.p, g + (size_t)c0 * h.nv, sizeof(double) * nc * (size_t)h.nv, cudaMemcpyHostToDevice,
                             st));
-    EB_CHECK(eb::mesh_apply(m, EB_PREC_FP64, 0, nd, nullptr, du.as<double>(), nullptr, dq.as<double>(), st));
+    EB_CHECK(eb::mesh_apply(m, precision, 0, nd, nullptr, du.as<double>(), nullptr, dq.as<double>(), st));
     EB_CUDA(cudaMemcpyAsync(b + (size_t)c0 * h.ne, dq.p, sizeof(double) * nc * (size_t)h.ne, cudaMemcpyDeviceToHost,
                             st));
   }

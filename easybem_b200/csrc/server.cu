@@ -325,7 +325,7 @@ class Server {
       std::vector<double> b;
       if (rc == EB_OK) {
         b.resize((size_t)r->nrhs * r->ne);
-        rc = eb_dirichlet_rhs(m, r->nrhs, r->g.data(), b.data());
+        rc = eb_dirichlet_rhs_prec(m, opt_.rhs_precision, r->nrhs, r->g.data(), b.data());
       }
       const double t2 = now_ms();
       if (rc == EB_OK && opt_.precond) rc = ensure_near_precond(eb_mesh_internal(m));
@@ -406,8 +406,11 @@ int eb_server_create(long long budget_bytes, int max_systems, const eb_solve_opt
     o.max_iterations = opt->max_iterations;
     o.inner_precision = opt->inner_precision;
     o.precond = opt->precond;
+    o.rhs_precision = opt->rhs_precision;
   }
   if (o.precond != 0 && o.precond != 1) return set_error(EB_ERR_INVALID, "precond must be 0 or 1");
+  if (o.rhs_precision != EB_PREC_FP64 && o.rhs_precision != EB_PREC_MIXED)
+    return set_error(EB_ERR_INVALID, "rhs_precision must be EB_PREC_FP64 or EB_PREC_MIXED");
   auto s = new eb_server_s();
   s->srv = std::make_unique<eb::Server>((size_t)budget_bytes, max_systems, o);
   *out = s;

@@ -481,6 +481,7 @@ static eb::SolveOptions to_options(const eb_solve_options* o)
     r.max_iterations = o->max_iterations;
     r.inner_precision = o->inner_precision;
     r.precond = o->precond;
+    r.rhs_precision = o->rhs_precision;
   }
   return r;
 }
@@ -498,6 +499,7 @@ void eb_solve_options_default(eb_solve_options* o)
   o->max_iterations = d.max_iterations;
   o->inner_precision = d.inner_precision;
   o->precond = d.precond;
+  o->rhs_precision = d.rhs_precision;
 }
 
 int eb_solver_create(const eb_solve_options* opt, eb_solver* out)

@@ -33,6 +33,7 @@ struct SolveOptions {
   int max_iterations = 4000;
   int inner_precision = EB_PREC_MIXED;
   int precond = 1;          // 1: near-field sparse approximate inverse (right), 0: none
+  int rhs_precision = EB_PREC_FP64;  // served right-hand sides (1/2 M + K) g
 };
 
 struct SolveStats {

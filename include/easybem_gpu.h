@@ -154,6 +154,13 @@ typedef struct eb_solve_options {
                         * triangles sharing a vertex with j); 0: none. It changes
                         * the iteration count only: every cycle ends with the
                         * true FP64 residual of V x = b. */
+  int rhs_precision;   /* the server's right-hand sides (1/2 M + K) g:
+                        * EB_PREC_FP64 (default) or EB_PREC_MIXED (FP32 far
+                        * field of K g, FP64 near field and mass term). For
+                        * data harmonic inside the surface 1/2 M g and K g
+                        * cancel (||K g|| / ||b|| ~ 20 on the serving tori), so
+                        * the 1e-7 error of the FP32 K g grows to a few 1e-6 in
+                        * b and the solution. The solvers take b as given. */
 } eb_solve_options;
 
 typedef struct eb_solve_stats {
@@ -227,6 +234,11 @@ int eb_server_stats(eb_server server, double* stats, int n);
  * matrix (src/BEM3dLaplace.cpp:448-486) and K the double layer, for nrhs
  * vertex data g ([nrhs][nnodes], host) into b ([nrhs][nelems], host). FP64. */
 int eb_dirichlet_rhs(eb_mesh mesh, int nrhs, const double* g, double* b);
+
+/* The same right-hand sides with K g in the given precision (EB_PREC_FP64 as
+ * eb_dirichlet_rhs, or EB_PREC_MIXED: FP32 far field, FP64 near field and
+ * mass term). No counterpart in the reference. */
+int eb_dirichlet_rhs_prec(eb_mesh mesh, int precision, int nrhs, const double* g, double* b);
 
 /* The quadrature rules behind index `order` (host only, no GPU needed):
  * the Gauss-Legendre rule on [0,1] (up to 64 points) and the triangle rule on

@@ -65,6 +65,27 @@ def test_requests_same_alone_and_in_mix(gpu_lib):
     srv.close()
 
 
+def test_mixed_rhs_precision_option(gpu_lib):
+    # mixed right-hand sides against FP64 ones (the default) for the same
+    # request: harmonic data make 1/2 M g and K g cancel (||K g|| / ||b|| of
+    # 18-26 here, condition number of V 133), so the FP32 error of K g shows in
+    # the solution at a few 1e-6 (measured 5.6e-6), not at 1e-7
+    nodes, elems, g = _request(32, 0.3, 3, 5)
+    out = {}
+    for prec in ("mixed", "fp64"):
+        srv = gpu_lib.Server(budget_bytes=8 << 30, rhs_precision=prec)
+        rid = srv.submit(nodes, elems, g)
+        _drain(srv, [rid])
+        t, stats, _ = srv.result(rid)
+        assert all(st["converged"] and st["rel_residual"] <= 1e-8 for st in stats)
+        out[prec] = t
+        srv.close()
+    for k in range(g.shape[0]):
+        assert rel_l2(out["mixed"][k], out["fp64"][k]) < 3e-5, k
+    with pytest.raises(ValueError):
+        gpu_lib.Server(budget_bytes=1 << 30, rhs_precision="fp16")
+
+
 def test_admission_respects_memory_budget(gpu_lib):
     reqs = [_request(64, 0.3, 2, s) for s in range(4)]
     probe = gpu_lib.Server(budget_bytes=64 << 30)

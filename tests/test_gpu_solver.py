@@ -162,3 +162,23 @@ def test_dirichlet_rhs_several_data_sets(gpu_lib, oracle):
             assert rel_l2(b, ref) < 1e-12, n
             for k in range(n):
                 assert rel_l2(b[k], ref[k]) < 1e-12, (n, k)
+            # K g with the FP32 far field (random data: no cancellation in b)
+            b32 = m.dirichlet_rhs(g, precision="mixed")
+            for k in range(n):
+                assert rel_l2(b32[k], ref[k]) < 1e-6, (n, k)
+
+
+def test_mixed_dirichlet_rhs_large_mesh(gpu_lib):
+    # 5,120 triangles (far field over many cells): the FP32 one- and
+    # four-column double-layer passes against the FP64 ones
+    nodes, elems = meshes.perturbed_icosphere(4, seed=2)
+    rng = np.random.default_rng(12)
+    with gpu_lib.Mesh(nodes, elems) as m:
+        for n in (1, 5):
+            g = rng.normal(size=(n, nodes.shape[0]))
+            b64 = m.dirichlet_rhs(g)
+            b32 = m.dirichlet_rhs(g, precision="mixed")
+            for k in range(n):
+                assert rel_l2(b32[k], b64[k]) < 1e-6, (n, k)
+            with pytest.raises(ValueError):
+                m.dirichlet_rhs(g, precision="fp16")

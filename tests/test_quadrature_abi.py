@@ -139,3 +139,23 @@ def test_plan_table_file_round_trip(tmp_path):
     with pytest.raises(eb.EasyBemError):
         eb.load_plans(str(tmp_path / "missing.txt"))
     eb.clear_plans()
+
+
+def test_solve_options_layout_and_defaults(ablib):
+    # the ctypes mirror of eb_solve_options must have the C layout: the
+    # library's defaults land in the right fields
+    from easybem_b200 import _lib
+    o = _lib.SolveOptions()
+    ablib.eb_solve_options_default(ctypes.byref(o))
+    assert (o.tol, o.inner_tol, o.restart, o.max_cycles, o.max_iterations) == (1e-8, 1e-6, 50, 40, 4000)
+    assert (o.inner_precision, o.precond, o.rhs_precision) == (_lib.EB_PREC_MIXED, 1, _lib.EB_PREC_FP64)
+
+
+def test_server_rejects_bad_rhs_precision_before_touching_the_gpu(ablib):
+    from easybem_b200 import _lib
+    o = _lib.SolveOptions()
+    ablib.eb_solve_options_default(ctypes.byref(o))
+    o.rhs_precision = 7
+    h = ctypes.c_void_p()
+    assert ablib.eb_server_create(1 << 30, 16, ctypes.byref(o), ctypes.byref(h)) == _lib.EB_ERR_INVALID
+    assert not h.value
