@@ -559,6 +559,15 @@ __device__ __forceinline__ void prep_point(const ApplyArgs& A, long long idx)
 // partial-sum reads of neighbouring rows contiguous; the row's original index
 // i = perm[s] addresses the near-field CSR and the outputs. Result: far sum
 // times J_i / (4 pi) plus the FP64 near field.
+//
+// The kernel is bound by memory latency, not bandwidth, unless each thread
+// keeps several loads in flight: the partial slots are read kFinPipe at a
+// time for every output at once, and the CSR columns and values of kFinPipe
+// entries are loaded before their densities are gathered. Each lane still
+// adds its terms in ascending slot / entry order, so the sums do not depend
+// on the grouping.
+constexpr int kFinPipe = 4;
+
 __device__ __forceinline__ double lanes_sum(double v)
 {
 #pragma unroll
@@ -566,45 +575,90 @@ __device__ __forceinline__ double lanes_sum(double v)
   return v;
 }
 
+__device__ __forceinline__ size_t partial_offset(const ApplyArgs& A, int k)
+{
+  if (A.nchunk == 1) return (size_t)k * A.nitems;
+  const int sp = k / A.nchunk;
+  return (size_t)sp * A.nitems + (k - sp * A.nchunk);
+}
+
+// nr[c] += sum over the lane's entries of val[k] * x_c[col[k]], c < NC
+template <int NC>
+__device__ __forceinline__ void near_rows(const int* __restrict__ col, const double* __restrict__ val, int kb, int ke,
+                                          const double* __restrict__ x, size_t xstride, int lane, double* nr)
+{
+  for (int k0 = kb + lane; k0 < ke; k0 += kFinPipe * kFinalizeLanes) {
+    int cj[kFinPipe];
+    double vj[kFinPipe];
+#pragma unroll
+    for (int r = 0; r < kFinPipe; ++r) {
+      const int k = k0 + r * kFinalizeLanes;
+      cj[r] = k < ke ? col[k] : -1;
+      vj[r] = k < ke ? val[k] : 0.0;
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      double xj[kFinPipe];
+#pragma unroll
+      for (int r = 0; r < kFinPipe; ++r) xj[r] = cj[r] >= 0 ? x[(size_t)c * xstride + cj[r]] : 0.0;
+#pragma unroll
+      for (int r = 0; r < kFinPipe; ++r)
+        if (cj[r] >= 0) nr[c] += vj[r] * xj[r];
+    }
+  }
+}
+
 template <int NSL, int ND>
 __device__ __forceinline__ void finalize_row(const ApplyArgs& A, int row_block)
 {
+  constexpr int NO = NSL + ND;
   const int lane = threadIdx.x % kFinalizeLanes;
   const int s = row_block * kFinalizeRows + threadIdx.x / kFinalizeLanes;
   // every lane of the warp takes part in the shuffles; rows past the end add zeros
   const bool on = s < A.ne && !(A.active && *A.active == 0);
-  const int i = on ? A.perm[s] : 0;
-  const double scale = on ? A.trin[s].w * (0.25 / M_PI) : 0.0;
-  const size_t stride = (size_t)A.nsplit * A.nitems;
-  const int nparts = A.nsplit * A.nchunk;
-  for (int c = 0; c < NSL; ++c) {
-    double far = 0.0, nr = 0.0;
-    if (on) {
-      for (int k = lane; k < nparts; k += kFinalizeLanes) {
-        const int sp = k / A.nchunk, ch = k - sp * A.nchunk;
-        far += A.partial[c * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
+  double far[NO], nr[NO];
+#pragma unroll
+  for (int c = 0; c < NO; ++c) far[c] = nr[c] = 0.0;
+  int i = 0;
+  double scale = 0.0;
+  if (on) {
+    i = A.perm[s];
+    scale = A.trin[s].w * (0.25 / M_PI);
+    // far partial sums of row s: slot k of output c at c*stride + offset(k) + s*nchunk
+    const size_t stride = (size_t)A.nsplit * A.nitems;
+    const double* base = A.partial + (size_t)s * A.nchunk;
+    const int nparts = A.nsplit * A.nchunk;
+    int k = lane;
+    for (; k + (kFinPipe - 1) * kFinalizeLanes < nparts; k += kFinPipe * kFinalizeLanes) {
+      double x[kFinPipe][NO];
+#pragma unroll
+      for (int r = 0; r < kFinPipe; ++r) {
+        const size_t off = partial_offset(A, k + r * kFinalizeLanes);
+#pragma unroll
+        for (int c = 0; c < NO; ++c) x[r][c] = base[c * stride + off];
       }
-      for (int k = A.sl_rowptr[i] + lane; k < A.sl_rowptr[i + 1]; k += kFinalizeLanes)
-        nr += A.sl_val[k] * A.t[(size_t)c * A.tstride + A.sl_col[k]];
+#pragma unroll
+      for (int r = 0; r < kFinPipe; ++r)
+#pragma unroll
+        for (int c = 0; c < NO; ++c) far[c] += x[r][c];
     }
-    far = lanes_sum(far);
-    nr = lanes_sum(nr);
-    if (on && lane == 0) A.v[(size_t)c * A.vstride + i] = scale * far + nr;
+    for (; k < nparts; k += kFinalizeLanes) {
+      const size_t off = partial_offset(A, k);
+#pragma unroll
+      for (int c = 0; c < NO; ++c) far[c] += base[c * stride + off];
+    }
+    // FP64 near field: SL rows gather t, DL rows gather u
+    if (NSL > 0) near_rows<NSL>(A.sl_col, A.sl_val, A.sl_rowptr[i], A.sl_rowptr[i + 1], A.t, A.tstride, lane, nr);
+    if (ND > 0) near_rows<ND>(A.dl_col, A.dl_val, A.dl_rowptr[i], A.dl_rowptr[i + 1], A.u, A.ustride, lane, nr + NSL);
   }
-  for (int c = 0; c < ND; ++c) {
-    double far = 0.0, nr = 0.0;
-    if (on) {
-      for (int k = lane; k < nparts; k += kFinalizeLanes) {
-        const int sp = k / A.nchunk, ch = k - sp * A.nchunk;
-        far += A.partial[(NSL + c) * stride + (size_t)sp * A.nitems + (size_t)s * A.nchunk + ch];
-      }
-      const double* u = A.u + (size_t)c * A.ustride;
-      for (int k = A.dl_rowptr[i] + lane; k < A.dl_rowptr[i + 1]; k += kFinalizeLanes)
-        nr += A.dl_val[k] * u[A.dl_col[k]];
+#pragma unroll
+  for (int c = 0; c < NO; ++c) {
+    const double f = lanes_sum(far[c]);
+    const double n = lanes_sum(nr[c]);
+    if (on && lane == 0) {
+      if (c < NSL) A.v[(size_t)c * A.vstride + i] = scale * f + n;
+      else A.q[(size_t)(c - NSL) * A.qstride + i] = scale * f + n;
     }
-    far = lanes_sum(far);
-    nr = lanes_sum(nr);
-    if (on && lane == 0) A.q[(size_t)c * A.qstride + i] = scale * far + nr;
   }
 }
 
