@@ -49,8 +49,8 @@ WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L{leve
 FMA_OPS_PER_PAIR = 8
 FLOPS_PER_PAIR = 2 * FMA_OPS_PER_PAIR
 RSQRT_PER_PAIR = 1
-# DRAM bytes (read + write) of one far-field launch on the L6 workload, from the ncu capture
-# summarised in profiles/far_kernel_f32_sl_dl_icosphere_L6.md (39.70 MB read + 1.36 MB written).
+# DRAM bytes (read + write) of one far-field launch on the L6 workload, from an ncu capture
+# of that launch (39.70 MB read + 1.36 MB written).
 FAR_TRAFFIC_L6 = 39.70e6 + 1.36e6
 
 

@@ -116,8 +116,8 @@ int autotune(Mesh* m, int precision, int operators, int reps, int* best_ips, int
   EB_CHECK(v.alloc(sizeof(double) * h.ne));
   EB_CHECK(u.alloc(sizeof(double) * h.nv));
   EB_CHECK(q.alloc(sizeof(double) * h.ne));
-  EB_CUDA(cudaMemcpy(t.p, ht.data(), sizeof(double) * h.ne, cudaMemcpyHostToDevice));
-  EB_CUDA(cudaMemcpy(u.p, hu.data(), sizeof(double) * h.nv, cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(t.p, ht.data(), sizeof(double) * h.ne));
+  EB_CHECK(copy_h2d(u.p, hu.data(), sizeof(double) * h.nv));
 
   cudaStream_t st = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;

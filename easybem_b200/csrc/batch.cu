@@ -14,7 +14,7 @@ int batch_entry_init(BatchEntry* e, Mesh* m)
   EB_CHECK(e->partial.alloc(sizeof(double) * (size_t)kBatchCols * m->plan.nsplit * h.nitems));
   EB_CHECK(e->tin.alloc(sizeof(double) * (size_t)kBatchCols * h.ne));
   EB_CHECK(e->vout.alloc(sizeof(double) * (size_t)kBatchCols * h.ne));
-  EB_CUDA(cudaMemset(e->tin.p, 0, e->tin.bytes));
+  EB_CHECK(memset_sync(e->tin.p, 0, e->tin.bytes));
   return EB_OK;
 }
 
@@ -85,15 +85,15 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   fin_blocks_ = foff[n];
 
   EB_CHECK(desc_.alloc(sizeof(FarMeshDesc) * n));
-  EB_CUDA(cudaMemcpy(desc_.p, desc.data(), sizeof(FarMeshDesc) * n, cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(desc_.p, desc.data(), sizeof(FarMeshDesc) * n));
   EB_CHECK(args_.alloc(sizeof(ApplyArgs) * n));
-  EB_CUDA(cudaMemcpy(args_.p, args.data(), sizeof(ApplyArgs) * n, cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(args_.p, args.data(), sizeof(ApplyArgs) * n));
   EB_CHECK(items_.alloc(sizeof(WorkItem) * flat.size()));
-  EB_CUDA(cudaMemcpy(items_.p, flat.data(), sizeof(WorkItem) * flat.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(items_.p, flat.data(), sizeof(WorkItem) * flat.size()));
   EB_CHECK(prep_off_.alloc(sizeof(int) * (n + 1)));
-  EB_CUDA(cudaMemcpy(prep_off_.p, poff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(prep_off_.p, poff.data(), sizeof(int) * (n + 1)));
   EB_CHECK(fin_off_.alloc(sizeof(int) * (n + 1)));
-  EB_CUDA(cudaMemcpy(fin_off_.p, foff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(fin_off_.p, foff.data(), sizeof(int) * (n + 1)));
   EB_CHECK(counter_.alloc(sizeof(int)));
 
   smem_ = far_smem_bytes(src_tile, Q_, rec_slots(nsl_, false), fp32);
@@ -187,7 +187,7 @@ int eb_batch_create(int nmesh, const eb_mesh* meshes, int ncols, int precision, 
   }
   EB_CHECK(b->flags.alloc(sizeof(int) * nmesh));
   std::vector<int> ones(nmesh, 1);
-  EB_CUDA(cudaMemcpy(b->flags.p, ones.data(), sizeof(int) * nmesh, cudaMemcpyHostToDevice));
+  EB_CHECK(eb::copy_h2d(b->flags.p, ones.data(), sizeof(int) * nmesh));
   EB_CHECK(b->batch.build(ents, precision == EB_PREC_MIXED, ncols, b->flags.as<int>()));
   EB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   *out = b.release();

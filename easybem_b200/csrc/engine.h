@@ -22,6 +22,14 @@ cudaError_t prep_launch_batch(bool fp32, int NSL, int ND, const ApplyArgs* d_arg
 cudaError_t finalize_launch_batch(int NSL, int ND, const ApplyArgs* d_args, const int* d_off, int n, int nblocks,
                                   cudaStream_t st);
 
+// Blocking set-up copies and memset on the calling thread's non-blocking
+// stream (host side through a pinned staging buffer): unlike cudaMemcpy and
+// cudaMemset they do not go through the legacy default stream. The current
+// device must own dst (or src).
+int copy_h2d(void* dst, const void* src, size_t bytes);
+int copy_d2h(void* dst, const void* src, size_t bytes);
+int memset_sync(void* dst, int value, size_t bytes);
+
 // Returns the pool memory of a device that no buffer uses to the driver
 // (waits for the device); the bytes the pool holds unused.
 int devmem_trim(int device);

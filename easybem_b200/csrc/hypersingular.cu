@@ -78,11 +78,11 @@ int ensure_vertex_lists(Mesh* m)
   for (int i = 0; i < h.ne; i++)
     for (int k = 0; k < 3; k++) vlist[fill[h.elems[3 * i + k]]++] = (i << 2) | k;
   EB_CHECK(m->vtri_ptr.alloc(sizeof(int) * vptr.size()));
-  EB_CUDA(cudaMemcpy(m->vtri_ptr.p, vptr.data(), sizeof(int) * vptr.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(m->vtri_ptr.p, vptr.data(), sizeof(int) * vptr.size()));
   EB_CHECK(m->vtri_list.alloc(sizeof(int) * vlist.size()));
-  EB_CUDA(cudaMemcpy(m->vtri_list.p, vlist.data(), sizeof(int) * vlist.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(m->vtri_list.p, vlist.data(), sizeof(int) * vlist.size()));
   EB_CHECK(m->elems0.alloc(sizeof(int) * h.elems.size()));
-  EB_CUDA(cudaMemcpy(m->elems0.p, h.elems.data(), sizeof(int) * h.elems.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(m->elems0.p, h.elems.data(), sizeof(int) * h.elems.size()));
   return EB_OK;
 }
 
@@ -99,7 +99,7 @@ static int ensure_curls(Mesh* m)
     triangle_curls(P[0], P[1], P[2], &curl[9 * (size_t)i]);
   }
   EB_CHECK(m->curl9.alloc(sizeof(double) * curl.size()));
-  EB_CUDA(cudaMemcpy(m->curl9.p, curl.data(), sizeof(double) * curl.size(), cudaMemcpyHostToDevice));
+  EB_CHECK(copy_h2d(m->curl9.p, curl.data(), sizeof(double) * curl.size()));
   EB_CHECK(m->hs_x.alloc(sizeof(double) * 3 * (size_t)h.ne));
   EB_CHECK(m->hs_w.alloc(sizeof(double) * 3 * (size_t)h.ne));
   return EB_OK;

@@ -21,9 +21,17 @@
 //
 // The first call on each device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call
-// before any stream capture.
+// before any stream capture. With CUDA's lazy module loading (the default)
+// the array is only placed in device memory at that first lookup, so the
+// first call on a device is where its 32 MiB are taken: make it (or one
+// warm-up call) at start-up, before the caller's own allocator fills the
+// device; if no room is left then, it returns EB_ERR_CUDA. The looked-up
+// address is kept for the life of the process, so after cudaDeviceReset the
+// library must be loaded again.
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
 #include <string>
 
 #include "engine.h"
@@ -35,7 +43,10 @@ constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-static void* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+// Device address of g_noalloc_scratch per device, looked up once under
+// g_noalloc_mu (calls from several host threads may race to the first lookup).
+static std::atomic<void*> g_noalloc_ptr[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mu;
 
 static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -63,8 +74,10 @@ extern "C" int eb_apply_sl_dl_noalloc(eb_mesh handle, int precision, const doubl
   if (!sl && !dl) return set_error(EB_ERR_INVALID, "nothing to apply: pass t/v and/or u/q");
   const int nsl = sl ? 1 : 0;
   const bool fp32 = precision == EB_PREC_MIXED;
+  if (m->device < 0 || m->device >= kNoAllocMaxDevices)
+    return set_error(EB_ERR_INVALID, "device index " + std::to_string(m->device) + " beyond the " +
+                                         std::to_string(kNoAllocMaxDevices) + " devices eb_apply_sl_dl_noalloc serves");
   EB_CUDA(cudaSetDevice(m->device));
-  if (m->device < 0 || m->device >= kNoAllocMaxDevices) return set_error(EB_ERR_INVALID, "device index too large");
 
   // scratch layout: [counter | descriptor | source records | partial sums]
   const int nrec = rec_slots(nsl, dl);
@@ -82,12 +95,16 @@ extern "C" int eb_apply_sl_dl_noalloc(eb_mesh handle, int precision, const doubl
                                          std::to_string(kNoAllocScratchBytes) + " bytes (use eb_apply_sl_dl_device)");
 
   // once per device, with that device current
-  if (!g_noalloc_ptr[m->device]) {
-    void* p = nullptr;
-    EB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_ptr[m->device] = p;
+  void* scratch = g_noalloc_ptr[m->device].load(std::memory_order_acquire);
+  if (!scratch) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    scratch = g_noalloc_ptr[m->device].load(std::memory_order_relaxed);
+    if (!scratch) {
+      EB_CUDA(cudaGetSymbolAddress(&scratch, g_noalloc_scratch));
+      g_noalloc_ptr[m->device].store(scratch, std::memory_order_release);
+    }
   }
-  unsigned char* base = static_cast<unsigned char*>(g_noalloc_ptr[m->device]);
+  unsigned char* base = static_cast<unsigned char*>(scratch);
   int* counter = reinterpret_cast<int*>(base);
   FarMeshDesc* d_desc = reinterpret_cast<FarMeshDesc*>(base + off_desc);
   void* rec = base + off_rec;

@@ -119,7 +119,7 @@ static int ensure_p1_near(Mesh* m)
   DevBuf d_nodes, d_elems, d_pi, d_pj, d_ent, d_cptr, d_contrib;
   auto up = [](DevBuf& b, const void* src, size_t bytes) -> int {
     EB_CHECK(b.alloc(std::max<size_t>(bytes, 16)));
-    if (bytes) EB_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+    if (bytes) EB_CHECK(copy_h2d(b.p, src, bytes));
     return EB_OK;
   };
   EB_CHECK(up(d_nodes, h.nodes.data(), sizeof(double) * h.nodes.size()));
@@ -171,7 +171,7 @@ int mesh_apply_sl_p1(Mesh* m, int precision, const double* d_t, double* d_v, cud
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
     EB_CHECK(var.desc.alloc(sizeof(FarMeshDesc)));
-    EB_CUDA(cudaMemcpy(var.desc.p, &desc, sizeof desc, cudaMemcpyHostToDevice));
+    EB_CHECK(copy_h2d(var.desc.p, &desc, sizeof desc));
     var.grid = std::min(nsm * occ, std::max(1, m->nitems_work));
     var.smem = smem;
     var.src_tile = desc.src_tile;

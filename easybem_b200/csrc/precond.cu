@@ -215,8 +215,9 @@ extern "C" int eb_apply_near_precond(eb_mesh mesh, const double* x, double* y)
   eb::DevBuf dx, dy;
   EB_CHECK(dx.alloc(bytes));
   EB_CHECK(dy.alloc(bytes));
-  EB_CUDA(cudaMemcpy(dx.p, x, bytes, cudaMemcpyHostToDevice));
+  EB_CHECK(eb::copy_h2d(dx.p, x, bytes));
   EB_CUDA(eb::near_precond_apply(m, dx.as<double>(), dy.as<double>(), nullptr));
-  EB_CUDA(cudaMemcpy(y, dy.p, bytes, cudaMemcpyDeviceToHost));
+  EB_CUDA(cudaStreamSynchronize(nullptr));  // the copy below runs on another stream
+  EB_CHECK(eb::copy_d2h(y, dy.p, bytes));
   return EB_OK;
 }

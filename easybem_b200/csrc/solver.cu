@@ -184,9 +184,9 @@ int SolverPool::add(Mesh* m, int nrhs, const double* b_host, int* ids)
       EB_CHECK(s->x.alloc(sizeof(double) * ne));
       EB_CHECK(s->b.alloc(sizeof(double) * ne));
       EB_CHECK(s->r.alloc(sizeof(double) * ne));
-      EB_CUDA(cudaMemset(s->x.p, 0, sizeof(double) * ne));
+      EB_CHECK(memset_sync(s->x.p, 0, sizeof(double) * ne));
       const double* bc = b_host + (size_t)c * ne;
-      EB_CUDA(cudaMemcpy(s->b.p, bc, sizeof(double) * ne, cudaMemcpyHostToDevice));
+      EB_CHECK(copy_h2d(s->b.p, bc, sizeof(double) * ne));
       double bn = 0.0;
       for (int i = 0; i < ne; i++) bn += bc[i] * bc[i];
       s->bnorm = std::sqrt(bn);
@@ -232,7 +232,7 @@ int SolverPool::rebuild()
   }
   const size_t n1 = std::max(S, 1);
   EB_CHECK(d_tab_.alloc(sizeof(SysDev) * n1));
-  if (S) EB_CUDA(cudaMemcpy(d_tab_.p, tab.data(), sizeof(SysDev) * S, cudaMemcpyHostToDevice));
+  if (S) EB_CHECK(copy_h2d(d_tab_.p, tab.data(), sizeof(SysDev) * S));
   EB_CHECK(d_phase_.alloc(sizeof(int) * n1));
   EB_CHECK(d_k_.alloc(sizeof(int) * n1));
   EB_CHECK(d_fresh_.alloc(sizeof(int) * n1));
@@ -423,7 +423,7 @@ int SolverPool::result(int id, double* x_host, SolveStats* stats)
 {
   for (auto& s : sys_)
     if (s->id == id) {
-      if (x_host) EB_CUDA(cudaMemcpy(x_host, s->x.p, sizeof(double) * s->ne, cudaMemcpyDeviceToHost));
+      if (x_host) EB_CHECK(copy_d2h(x_host, s->x.p, sizeof(double) * s->ne));
       if (stats) {
         stats->converged = s->converged ? 1 : 0;
         stats->cycles = s->cycles;

@@ -91,7 +91,10 @@ int eb_apply_sl_dl_device(eb_mesh mesh, int precision, const double* d_t, const 
  * loading the library keeps until exit. Meshes needing more scratch are
  * rejected (EB_ERR_INVALID, message gives the size). Calls share that array:
  * calls overlapping on the GPU race. The first call on a device looks up the
- * array's address and should come before any stream capture. */
+ * array's address and should come before any stream capture; under CUDA's
+ * lazy module loading (the default) that first call is also where the 32 MiB
+ * are placed on the device, so make it at start-up, before the caller's own
+ * allocator fills the device (no room then: EB_ERR_CUDA). */
 int eb_apply_sl_dl_noalloc(eb_mesh mesh, int precision, const double* d_t, const double* d_u,
                            double* d_v, double* d_q, void* stream);
 

@@ -37,9 +37,29 @@ def _i(a):
     return a.ctypes.data_as(_ip)
 
 
+def reference_root():
+    """The reference source tree, if one is available to build from.
+
+    Taken from the environment variable ``EASYBEM_REFERENCE``, else a checkout
+    named ``reference`` beside this repository's directory; None when neither
+    holds ``src/BEM3dLaplace.cpp`` (the GPU box carries only the prebuilt
+    ``_ref`` libraries).
+    """
+    cands = [os.environ.get("EASYBEM_REFERENCE", ""),
+             os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for c in cands:
+        if c and os.path.isfile(os.path.join(c, "src", "BEM3dLaplace.cpp")):
+            return os.path.abspath(c)
+    return None
+
+
 def build():
-    """Compiles the port (and the reference library when its sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    """Compiles the port (and the reference libraries when its sources exist)."""
+    cmd = ["make", "-s", "-C", HERE, "all"]
+    ref = reference_root()
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True)
 
 
 def ref_available() -> bool:

@@ -13,6 +13,17 @@ Writes
   561-781) on small meshes, and V t, K u for seeded densities, at several
   quadrature indices, plus evaluateLaplace3d (:784-843) at seeded points. The cube is the reference example mesh
   python/examples/cube01-surface.txt (8 vertices, 12 triangles).
+* ``reference_orders.npz``: the meshes and quadrature indices the reference's
+  own GPU driver runs (python/examples/laplace3dDirichletGPU.py:22-25, :30-35,
+  :62: shaft-surface_verycoarse.vol scaled by 1/100, refined 1->4 per step,
+  indices 9 + step) and its Neumann driver (laplace3dNeumannGPU.py:12-22:
+  the same mesh refined once, index 4), plus index 7 on the perturbed
+  icosphere, index 18 (the largest rule) on the cube, and sampled rows of the
+  10,722-triangle shaft-surface.txt. V t, K u (and D u at index 4) come from
+  the reference's dense getLaplace3d, or from its pair routines row by row
+  (``rows`` arrays) where the dense matrices would be large.
+
+``python tests/golden/make_golden.py orders`` rewrites only the second file.
 """
 from __future__ import annotations
 
@@ -28,7 +39,13 @@ sys.path.insert(0, ROOT)
 from easybem_b200 import meshes  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REF_CUBE = "/root/reference/python/examples/cube01-surface.txt"
+
+def ref_example(name):
+    """A mesh file of the reference's python/examples directory."""
+    root = O.reference_root()
+    if root is None:
+        raise SystemExit("reference tree not found: set EASYBEM_REFERENCE")
+    return os.path.join(root, "python", "examples", name)
 
 
 def compact(nodes, elems1):
@@ -57,9 +74,64 @@ def two_spheres():
     return np.vstack([v, w]), np.vstack([f, f + v.shape[0]]).astype(np.int32)
 
 
+def orders_cases():
+    """Fixtures at the reference drivers' own meshes and quadrature indices."""
+    out = {}
+
+    def dense_case(name, nodes, elems, orders, hyper_at=()):
+        rng = np.random.default_rng(17)
+        t = rng.normal(size=elems.shape[0])
+        u = rng.normal(size=nodes.shape[0])
+        out[f"{name}_nodes"], out[f"{name}_elems"] = nodes, elems
+        out[f"{name}_t"], out[f"{name}_u"] = t, u
+        out[f"{name}_orders"] = np.array(orders)
+        for o in orders:
+            V, K, D, M = O.ref_dense(nodes, elems, o)
+            out[f"{name}_o{o}_Vt"] = V @ t
+            out[f"{name}_o{o}_Ku"] = K @ u
+            if o in hyper_at:
+                out[f"{name}_o{o}_Du"] = D @ u
+                out[f"{name}_o{o}_Mu"] = M @ u
+
+    def rows_case(name, nodes, elems, order, rows):
+        rng = np.random.default_rng(19)
+        t = rng.normal(size=elems.shape[0])
+        u = rng.normal(size=nodes.shape[0])
+        out[f"{name}_nodes"], out[f"{name}_elems"] = nodes, elems
+        out[f"{name}_t"], out[f"{name}_u"] = t, u
+        out[f"{name}_orders"] = np.array([order])
+        out[f"{name}_rows"] = rows.astype(np.int32)
+        v, q = O.ref_apply_rows(nodes, elems, t, u, rows=rows, order=order)
+        out[f"{name}_o{order}_Vt"] = v
+        out[f"{name}_o{order}_Ku"] = q
+
+    P, T, _ = meshes.load_netgen_vol(ref_example("shaft-surface_verycoarse.vol"))
+    P = P / 100.0  # laplace3dDirichletGPU.py:33
+    T = T.astype(np.int32)
+    dense_case("shaft0", P, T, [4, 9, 10, 11, 12, 13])
+    P1, T1 = meshes.refine_mesh(P, T)[:2]
+    T1 = T1.astype(np.int32)
+    dense_case("shaft1", P1, T1, [4, 10], hyper_at=(4,))
+    P2, T2 = meshes.refine_mesh(P1, T1)[:2]
+    T2 = T2.astype(np.int32)
+    rows_case("shaft2", P2, T2, 11, np.arange(0, T2.shape[0], 34))
+    v, f = meshes.perturbed_icosphere(2, seed=3)
+    dense_case("pico2", v, f.astype(np.int32), [7])
+    cube_nodes, cube_elems, _ = meshes.load_surface_txt(ref_example("cube01-surface.txt"))
+    dense_case("cube", cube_nodes, cube_elems.astype(np.int32), [18])
+    S, ST, _ = meshes.load_surface_txt(ref_example("shaft-surface.txt"))
+    S = S / 100.0
+    ST = ST.astype(np.int32)
+    rows_case("shafttxt", S, ST, 4, np.random.default_rng(23).choice(ST.shape[0], 256, replace=False))
+    np.savez_compressed(os.path.join(HERE, "reference_orders.npz"), **out)
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libeasybem_ref.so is missing: run `make -C oracle ref` first")
+    if sys.argv[1:] == ["orders"]:
+        orders_cases()
+        return
     lib = O.ref_lib()
     tabs = {}
     for o in range(20):
@@ -75,7 +147,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "reference_quadrature.npz"), **tabs)
 
     cases = {}
-    cube_nodes, cube_elems, _ = meshes.load_surface_txt(REF_CUBE)
+    cube_nodes, cube_elems, _ = meshes.load_surface_txt(ref_example("cube01-surface.txt"))
     cases["cube"] = (cube_nodes, cube_elems, [4])
     v, f = meshes.icosphere(2)
     cases["ico2"] = (v, f, [4])
@@ -117,6 +189,7 @@ def main():
                 out[f"{name}_pts"] = pts
                 out[f"{name}_eval"] = O.ref_evaluate(nodes, elems, pts, t, u, 4)
     np.savez_compressed(os.path.join(HERE, "reference_ops.npz"), **out)
+    orders_cases()
     print("wrote", sorted(os.listdir(HERE)))
 
 

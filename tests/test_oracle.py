@@ -129,3 +129,29 @@ def test_p1_single_layer_formulas_sum_to_pinned_p0(oracle):
     V1 = oracle.p1_dense(nodes, elems)
     assert np.linalg.norm(V1 - V1.T) / np.linalg.norm(V1) < 1e-6
     assert np.linalg.eigvalsh(0.5 * (V1 + V1.T)).min() > 0
+
+
+def test_oracle_matches_golden_at_reference_driver_orders(oracle):
+    """The port against the reference's outputs at the reference drivers' own
+    meshes and indices (tests/golden/reference_orders.npz): every 5th row
+    of each dense case, all stored rows of the sampled ones."""
+    import os
+
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "reference_orders.npz"))
+    cases = [("shaft0", o) for o in (4, 9, 10, 11, 12, 13)] + [
+        ("shaft1", 4), ("shaft1", 10), ("shaft2", 11), ("pico2", 7), ("cube", 18), ("shafttxt", 4)]
+    for name, o in cases:
+        nodes, elems, t, u = z[f"{name}_nodes"], z[f"{name}_elems"], z[f"{name}_t"], z[f"{name}_u"]
+        vg, qg = z[f"{name}_o{o}_Vt"], z[f"{name}_o{o}_Ku"]
+        if f"{name}_rows" in z:
+            rows = z[f"{name}_rows"]
+            sel = np.arange(rows.size)
+        else:
+            rows = np.arange(0, elems.shape[0], 5, dtype=np.int32)
+            sel = rows
+        oracle.set_order(o)
+        v, q = oracle.apply_rows(nodes, elems, t, u, rows)
+        assert rel_l2(v, vg[sel]) < 1e-13, (name, o)
+        assert rel_l2(q, qg[sel]) < 1e-13, (name, o)
+    oracle.set_order(4)

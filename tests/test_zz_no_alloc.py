@@ -8,8 +8,10 @@ because it can synchronise the device. Such a caller hands in device buffers
 it already owns; the entry point keeps its scratch in a fixed device array.
 
 Checked here: two calls in a row agree with the allocating entry point
-(eb_apply_sl_dl_device) on the same inputs, in both precisions, and a mesh
-whose scratch exceeds the fixed array is refused with a clear error.
+(eb_apply_sl_dl_device) on the same inputs, in both precisions; after one
+warm-up call, further calls change neither the device's free memory nor the
+library's memory pool nor torch's caching allocator; and a mesh whose scratch
+exceeds the fixed array is refused with a clear error.
 """
 import ctypes
 
@@ -57,6 +59,36 @@ def test_noalloc_matches_allocating_apply_twice(gpu_lib, precision, tol):
         torch.cuda.synchronize()
         assert rel_l2(v.cpu().numpy(), v_sl.cpu().numpy()) <= tol
         assert torch.all(q == 7.0)
+
+
+def test_noalloc_calls_take_no_device_memory(gpu_lib):
+    import torch
+
+    from easybem_b200 import _lib, meshes
+    L = _lib.lib()
+    nodes, elems = meshes.perturbed_icosphere(4, seed=11)
+    rng = np.random.default_rng(5)
+    t = torch.from_numpy(rng.normal(size=elems.shape[0])).cuda()
+    u = torch.from_numpy(rng.normal(size=nodes.shape[0])).cuda()
+    v = torch.empty_like(t)
+    q = torch.empty_like(t)
+    cached = ctypes.c_longlong(0)
+    with gpu_lib.Mesh(nodes, elems) as m:
+        # the first call on the device places the fixed array (lazy module loading)
+        _lib.check(L.eb_apply_sl_dl_noalloc(m.handle, 1, _ptr(t), _ptr(u), _ptr(v), _ptr(q), None))
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        reserved0 = torch.cuda.memory_reserved()
+        _lib.check(L.eb_cached_memory_bytes(ctypes.byref(cached)))
+        pool0 = cached.value
+        for precision in (1, 0, 1, 0):
+            _lib.check(L.eb_apply_sl_dl_noalloc(m.handle, precision, _ptr(t), _ptr(u), _ptr(v), _ptr(q), None))
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        _lib.check(L.eb_cached_memory_bytes(ctypes.byref(cached)))
+        assert free1 == free0
+        assert torch.cuda.memory_reserved() == reserved0
+        assert cached.value == pool0
 
 
 def test_noalloc_rejects_meshes_beyond_its_scratch(gpu_lib):
