@@ -70,8 +70,11 @@ def parse_args(argv=None):
                         "torus solves, p50/p99 latency; large: icosphere L7 apply and solve; small: "
                         "icosphere L3 Dirichlet solve")
     p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
-    p.add_argument("--serve-sample", type=int, default=32,
+    p.add_argument("--serve-sample", type=int, default=300,
                    help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="matvec: skip the batch (256 ellipsoids), large (L7) and small (L3 solve) records "
+                        "that a one-GPU run adds to its line")
     p.add_argument("--rhs-precision", default="fp64", choices=["mixed", "fp64"],
                    help="serve: precision of the served right-hand sides (1/2 M + K) g")
     return p.parse_args(argv)
@@ -249,66 +252,109 @@ def run_serve(args):
         print(json.dumps(line), flush=True)
 
 
-def run_batch(args):
-    """256 closed surfaces (icosphere L2-L5 ellipsoids) x 4 RHS: batched applies and solves."""
+def batch_record(local, solves=True):
+    """256 closed surfaces (icosphere L2-L5 ellipsoids): batched SL+DL applies in
+    both precisions (one density pair per mesh, one persistent launch), the
+    4-RHS batched SL apply, and the GMRES-IR solves of all 1,024 systems."""
     import torch
     import easybem_b200 as eb
     from easybem_b200 import meshes
-    _, _, local = dist_env()
-    torch.cuda.set_device(local)
     items = meshes.ellipsoid_batch(256, seed=3, levels=(2, 3, 4, 5), nrhs=4)
     t0 = time.perf_counter()
     ms = [eb.Mesh(it["nodes"], it["elems"]) for it in items]
     t_create = time.perf_counter() - t0
-    rhs = [m.dirichlet_rhs(np.stack([1.0 / np.linalg.norm(it["nodes"] - p, axis=1) for p in it["sources"]]))
-           for m, it in zip(ms, items)]
     dev = torch.device("cuda", local)
-    d_t = [torch.from_numpy(np.ascontiguousarray(b)).to(dev) for b in rhs]
+    st = torch.cuda.current_stream()
+    rng = np.random.default_rng(41)
+    d_t = [torch.from_numpy(rng.normal(size=m.nelems)).to(dev) for m in ms]
+    d_u = [torch.from_numpy(rng.normal(size=it["nodes"].shape[0])).to(dev) for it in items]
     d_v = [torch.empty_like(x) for x in d_t]
-    out = {}
-    for prec in ("mixed", "fp64"):
-        bt = eb.Batch(ms, 4, prec)
-        st = torch.cuda.current_stream()
-        for _ in range(2):
-            bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v], st.cuda_stream)
-        k = 3 if prec == "mixed" else 2
+    d_q = [torch.empty_like(x) for x in d_t]
+    ptrs = lambda xs: [x.data_ptr() for x in xs]
+
+    def time_batch(bt, run, k):
+        for _ in range(2):  # the first call captures the graph
+            run(bt)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         a.record(st)
         for _ in range(k):
-            bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v], st.cuda_stream)
+            run(bt)
         b.record(st)
         torch.cuda.synchronize()
-        ms_apply = a.elapsed_time(b) / k
-        out[prec] = {"ms_per_apply": ms_apply, "Gpairs_per_s": bt.quad_pairs / (ms_apply * 1e-3) / 1e9,
-                     "rhs_evals_per_s_G": 4 * bt.quad_pairs / (ms_apply * 1e-3) / 1e9}
+        return a.elapsed_time(b) / k
+
+    out = {}
+    for prec in ("mixed", "fp64"):
+        bt = eb.Batch(ms, precision=prec, sl_dl=True)
+        ms_apply = time_batch(bt, lambda b: b.apply_sl_dl_device(ptrs(d_t), ptrs(d_u), ptrs(d_v), ptrs(d_q),
+                                                                  st.cuda_stream), 3 if prec == "mixed" else 2)
+        out[prec] = {"ms_per_apply": ms_apply, "Gpairs_per_s": bt.quad_pairs / (ms_apply * 1e-3) / 1e9}
+        out[prec + "_vq"] = (torch.cat(d_v).cpu().numpy(), torch.cat(d_q).cpu().numpy())
         bt.close()
-    t0 = time.perf_counter()
-    res = eb.solve(list(zip(ms, rhs)), tol=1e-8)
-    t_solve = time.perf_counter() - t0
-    stats = [s for _, sl in res for s in sl]
-    line = {"metric": METRIC, "workload": "batch", "value": out["mixed"]["Gpairs_per_s"], "unit": "Gpairs/s",
-            "higher_is_better": True, "data": "synthetic",
-            "config": {"workload": "256 ellipsoids (icosphere L2-L5, 320-20,480 triangles), 4 RHS each, "
-                                   "batched SL apply + GMRES(50)-IR to 1e-8",
-                       "quad_pairs_per_apply": int(sum(m.far_quad_pairs for m in ms))},
-            "apply_mixed": out["mixed"], "apply_fp64": out["fp64"],
-            "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
-            "mesh_setup_s": t_create, "solve_s": t_solve, "systems": len(stats),
-            "solves_per_s": len(stats) / t_solve, "converged": sum(s["converged"] for s in stats),
-            "max_rel_residual": max(s["rel_residual"] for s in stats),
-            "iterations_mean": float(np.mean([s["iterations"] for s in stats])),
-            "cycles_mean": float(np.mean([s["cycles"] for s in stats]))}
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    mixed_vs_fp64 = {"sl": rel(out["mixed_vq"][0], out["fp64_vq"][0]), "dl": rel(out["mixed_vq"][1], out["fp64_vq"][1])}
+    # sampled rows of 8 meshes against the CPU oracle
+    from oracle.oracle import Oracle
+    orc = Oracle(ORDER)
+    offs = np.cumsum([0] + [m.nelems for m in ms])
+    ev, eq = [], []
+    for i in range(0, 256, 32):
+        rows = np.sort(rng.choice(ms[i].nelems, 8, replace=False)).astype(np.int32)
+        vo, qo = orc.apply_rows(items[i]["nodes"], items[i]["elems"], d_t[i].cpu().numpy(), d_u[i].cpu().numpy(), rows)
+        ev.append((out["fp64_vq"][0][offs[i] + rows], out["mixed_vq"][0][offs[i] + rows], vo))
+        eq.append((out["fp64_vq"][1][offs[i] + rows], out["mixed_vq"][1][offs[i] + rows], qo))
+    cat = lambda L, k: np.concatenate([x[k] for x in L])
+    err = {"fp64_sl": rel(cat(ev, 0), cat(ev, 2)), "mixed_sl": rel(cat(ev, 1), cat(ev, 2)),
+           "fp64_dl": rel(cat(eq, 0), cat(eq, 2)), "mixed_dl": rel(cat(eq, 1), cat(eq, 2)), "oracle_rows": 64,
+           "mixed_vs_fp64_full": mixed_vs_fp64}
+    # 4 SL right-hand sides per mesh (the Dirichlet data of the solves)
+    rhs = [m.dirichlet_rhs(np.stack([1.0 / np.linalg.norm(it["nodes"] - p, axis=1) for p in it["sources"]]))
+           for m, it in zip(ms, items)]
+    d_b = [torch.from_numpy(np.ascontiguousarray(b)).to(dev) for b in rhs]
+    d_w = [torch.empty_like(x) for x in d_b]
+    bt = eb.Batch(ms, 4, "mixed")
+    ms4 = time_batch(bt, lambda b: b.apply_device(ptrs(d_b), ptrs(d_w), st.cuda_stream), 3)
+    pairs = bt.quad_pairs
+    bt.close()
+    rec = {"workload": "256 ellipsoids (icosphere L2-L5, 320-20,480 triangles), SL+DL batched apply "
+                       "(one density pair per mesh), 4-RHS SL batched apply, GMRES(50)-IR to 1e-8",
+           "quad_pairs_per_apply": int(pairs), "mesh_setup_s": t_create,
+           "sl_dl_mixed": out["mixed"], "sl_dl_fp64": out["fp64"],
+           "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
+           "rel_err_vs_oracle": err,
+           "sl_4rhs_mixed": {"ms_per_apply": ms4, "Gpairs_per_s": pairs / (ms4 * 1e-3) / 1e9,
+                             "rhs_evals_per_s_G": 4 * pairs / (ms4 * 1e-3) / 1e9}}
+    if solves:
+        t0 = time.perf_counter()
+        res = eb.solve(list(zip(ms, rhs)), tol=1e-8)
+        t_solve = time.perf_counter() - t0
+        stats = [x for _, sl in res for x in sl]
+        rec["solves"] = {"systems": len(stats), "seconds": t_solve, "solves_per_s": len(stats) / t_solve,
+                         "converged": sum(x["converged"] for x in stats),
+                         "max_rel_residual": max(x["rel_residual"] for x in stats),
+                         "iterations_mean": float(np.mean([x["iterations"] for x in stats])),
+                         "cycles_mean": float(np.mean([x["cycles"] for x in stats]))}
+    for m in ms:
+        m.close()
+    return rec
+
+
+def run_batch(args):
+    import torch
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    rec = batch_record(local)
+    line = {"metric": METRIC, "workload": "batch", "value": rec["sl_dl_mixed"]["Gpairs_per_s"], "unit": "Gpairs/s",
+            "higher_is_better": True, "data": "synthetic", "config": {"workload": rec.pop("workload")}, **rec}
     print(json.dumps(line), flush=True)
 
 
-def run_large(args):
-    """Icosphere L7 (327,680 triangles): SL+DL apply in both precisions and a GMRES-IR solve."""
-    import torch
+def large_record(local, solve=False):
+    """Icosphere L7 (327,680 triangles): SL+DL apply in both precisions, error on
+    16 oracle rows, optionally the GMRES-IR solve."""
     import easybem_b200 as eb
     from oracle.oracle import Oracle
-    _, _, local = dist_env()
-    torch.cuda.set_device(local)
     nodes, elems, t, u = make_problem(7)
     t0 = time.perf_counter()
     m = eb.Mesh(nodes, elems)
@@ -324,37 +370,48 @@ def run_large(args):
     rows = np.sort(rng.choice(elems.shape[0], 16, replace=False)).astype(np.int32)
     vo, qo = Oracle(ORDER).apply_rows(nodes, elems, t, u, rows)
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
-    g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
-    b = m.dirichlet_rhs(g)
-    t0 = time.perf_counter()
-    [(x, st)] = eb.solve([(m, b)], tol=1e-8)
-    t_solve = time.perf_counter() - t0
     pairs = m.far_quad_pairs
-    line = {"metric": METRIC, "workload": "large", "value": pairs / (res["mixed"][2] * 1e-3) / 1e9,
-            "unit": "Gpairs/s", "higher_is_better": True, "data": "synthetic",
-            "config": {"workload": "radius-perturbed icosphere L7 (327,680 triangles, 163,842 vertices)",
-                       "quad_pairs_per_step": pairs, "near_pairs": m.near_pairs},
-            "mesh_setup_s": t_create,
-            "mixed": {"far_ms": res["mixed"][2], "finalize_ms": res["mixed"][3]},
-            "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
-                     "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
-            "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed"][0][rows], vo), "mixed_dl": rel(res["mixed"][1][rows], qo),
-                                  "fp64_sl": rel(res["fp64"][0][rows], vo), "fp64_dl": rel(res["fp64"][1][rows], qo),
-                                  "oracle_rows": len(rows)},
-            "solve": {"seconds": t_solve, **st[0]}}
+    peak_tflops, peak_rsqrt = _measure_peak()
+    rate = pairs / (res["mixed"][2] * 1e-3)
+    bound = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
+    rec = {"workload": "radius-perturbed icosphere L7 (327,680 triangles, 163,842 vertices)",
+           "quad_pairs_per_step": pairs, "near_pairs": m.near_pairs, "mesh_setup_s": t_create,
+           "mixed": {"far_ms": res["mixed"][2], "finalize_ms": res["mixed"][3], "Gpairs_per_s": rate / 1e9,
+                     "fma_pipe_frac": rate * FLOPS_PER_PAIR / (peak_tflops * 1e12), "frac_of_pair_bound": rate / bound},
+           "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
+                    "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
+           "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed"][0][rows], vo), "mixed_dl": rel(res["mixed"][1][rows], qo),
+                                 "fp64_sl": rel(res["fp64"][0][rows], vo), "fp64_dl": rel(res["fp64"][1][rows], qo),
+                                 "oracle_rows": len(rows)}}
+    rec["mixed_over_fp64"] = rec["mixed"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
+    if solve:
+        g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
+        b = m.dirichlet_rhs(g)
+        t0 = time.perf_counter()
+        [(x, st)] = eb.solve([(m, b)], tol=1e-8)
+        rec["solve"] = {"seconds": time.perf_counter() - t0, **st[0]}
+    m.close()
+    return rec
+
+
+def run_large(args):
+    import torch
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    rec = large_record(local, solve=True)
+    line = {"metric": METRIC, "workload": "large", "value": rec["mixed"]["Gpairs_per_s"], "unit": "Gpairs/s",
+            "higher_is_better": True, "data": "synthetic", "config": {"workload": rec.pop("workload")}, **rec}
     print(json.dumps(line), flush=True)
 
 
-def run_small(args):
+def small_record(local):
     """Icosphere L3 (1,280 triangles): Dirichlet solve, g = 1/|x - (0,0,3)|, checked against the reference."""
-    import torch
     import easybem_b200 as eb
     from easybem_b200 import meshes
     from oracle import oracle as O
-    _, _, local = dist_env()
-    torch.cuda.set_device(local)
     nodes, elems = meshes.icosphere(3)
     g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
+
     def once():
         t0 = time.perf_counter()
         m = eb.Mesh(nodes, elems)
@@ -366,19 +423,29 @@ def run_small(args):
     m.close()
     t_gpu, m, x, st = once()
     rel = lambda a, c: float(np.linalg.norm(a - c) / np.linalg.norm(c))
-    line = {"metric": METRIC, "workload": "small", "value": 1e3 * t_gpu, "unit": "ms (mesh + RHS + solve)",
-            "higher_is_better": False, "data": "synthetic",
-            "config": {"workload": "unit icosphere L3 (1,280 triangles), Dirichlet g = 1/|x-(0,0,3)|"},
-            "cold_ms": 1e3 * t_cold, "solve": st[0]}
+    rec = {"workload": "unit icosphere L3 (1,280 triangles, 642 vertices), Dirichlet g = 1/|x-(0,0,3)|, "
+                       "mesh + right-hand side + GMRES-IR solve to 1e-8",
+           "ms": 1e3 * t_gpu, "cold_ms": 1e3 * t_cold, "solve": st[0]}
     rng = np.random.default_rng(0)
     dens = rng.normal(size=elems.shape[0])
     if O.ref_available():
         t0 = time.perf_counter()
         V, K, D, M = O.ref_dense(nodes, elems, ORDER)
         x_ref = np.linalg.solve(V, (0.5 * M + K) @ g)
-        line["reference_cpu_dense_s"] = time.perf_counter() - t0
-        line["rel_err_solution_vs_reference"] = rel(x, x_ref)
-        line["rel_err_matvec_vs_reference"] = rel(m.apply_sl(dens), V @ dens)
+        rec["reference_cpu_dense_s"] = time.perf_counter() - t0
+        rec["rel_err_solution_vs_reference"] = rel(x, x_ref)
+        rec["rel_err_matvec_vs_reference"] = rel(m.apply_sl(dens), V @ dens)
+    m.close()
+    return rec
+
+
+def run_small(args):
+    import torch
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    rec = small_record(local)
+    line = {"metric": METRIC, "workload": "small", "value": rec["ms"], "unit": "ms (mesh + RHS + solve)",
+            "higher_is_better": False, "data": "synthetic", "config": {"workload": rec.pop("workload")}, **rec}
     print(json.dumps(line), flush=True)
 
 
@@ -516,8 +583,17 @@ def main():
     nb = ctypes.c_longlong()
     _lib.check(L.eb_mesh_finalize_bytes(mesh.handle, ctypes.byref(nb)))
     near_bytes = nb.value  # near-field CSR + gathered densities + far partial sums + outputs
+    nb_spmv, nb_fold = ctypes.c_longlong(), ctypes.c_longlong()
+    _lib.check(L.eb_mesh_near_field_bytes(mesh.handle, ctypes.byref(nb_spmv), ctypes.byref(nb_fold)))
     cpu = None if args.no_cpu_baseline else cpu_reference_sample(nodes, elems, t, u)
     clocks = sampler.summary()
+    extras = {}
+    if world == 1 and not args.no_extras:
+        torch.cuda.synchronize()
+        for name, fn in (("small", small_record), ("batch", batch_record), ("large", large_record)):
+            a = time.perf_counter()
+            extras[name] = fn(local)
+            extras[name]["record_wall_s"] = time.perf_counter() - a
     serve = None
     if args.serve_sample > 0 and world == 1:
         from easybem_b200.serving import run_stream
@@ -550,6 +626,10 @@ def main():
                                     "(8 FMA-pipe ops = 16 flops and 1 rsqrt per quadrature pair)"},
         "near_field": {"kernel": "finalize_kernel<1,1> (near-field SpMV + partial-sum fold)",
                        "finalize_ms": fin_avg, "algorithmic_bytes": near_bytes,
+                       "spmv_bytes": nb_spmv.value, "fold_bytes": nb_fold.value,
+                       "note": "one launch does both the SL+DL near-field SpMV (spmv_bytes: CSR row pointers, "
+                               "columns, values, gathered densities, outputs) and the fold of the far-field "
+                               "partial sums (fold_bytes); GB/s counts both over the launch's event time",
                        "GB/s": near_bytes / (fin_avg * 1e-3) / 1e9 if fin_avg > 0 else None,
                        "hbm_peak_GB/s": _hbm_peak(), "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
         "clocks": clocks,
@@ -558,10 +638,16 @@ def main():
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if serve is not None:
         line["serve_sample"] = {"requests": serve["requests"], "p50_ms": serve["p50_ms"], "p99_ms": serve["p99_ms"],
-                                "solves_per_s": serve["solves_per_s"], "converged": serve["converged"],
-                                "max_rel_residual": serve["max_rel_residual"], "rhs_precision": args.rhs_precision,
-                                "note": "first requests of the 2,000-request Poisson stream (200/s); "
+                                "p50_solve_ms": serve["p50_solve_ms"], "p99_solve_ms": serve["p99_solve_ms"],
+                                "p99_queue_ms": serve["p99_queue_ms"], "wall_s": serve["wall_s"],
+                                "solves_per_s": serve["solves_per_s"], "rhs_per_s": serve["rhs_per_s"],
+                                "converged": serve["converged"], "right_hand_sides": serve["right_hand_sides"],
+                                "max_rel_residual": serve["max_rel_residual"], "iterations_mean": serve["iterations_mean"],
+                                "rhs_precision": args.rhs_precision, "server": serve["server"],
+                                "note": "first requests of the 2,000-request Poisson stream (200/s, 120 GB budget); "
                                         "full stream: bench.py --workload serve"}
+    for name, rec in extras.items():
+        line[name] = rec
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -209,20 +209,63 @@ def clear_plans():
     check(lib().eb_plan_table_clear())
 
 
-class Batch:
-    """P0 single-layer applies of many meshes x ncols right-hand sides in one launch.
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
 
+
+def read_surface(path: str):
+    """Reads a mesh file through the C ABI: easybem's plain-text surface
+    (``.txt``) or the surface triangles of a Netgen ``.vol`` file. Returns
+    (nodes [n,3] float64, elems [m,3] int32 1-based, labels [m] int32)."""
+    fn = lib().eb_read_netgen_vol if str(path).lower().endswith(".vol") else lib().eb_read_surface_txt
+    n, m = ctypes.c_int(), ctypes.c_int()
+    p = os.fsencode(str(path))
+    check(fn(p, ctypes.byref(n), None, ctypes.byref(m), None, None))
+    nodes = np.empty((n.value, 3))
+    elems = np.empty((m.value, 3), dtype=np.int32)
+    labels = np.empty(m.value, dtype=np.int32)
+    check(fn(p, ctypes.byref(n), _ptr(nodes), ctypes.byref(m), _ptr(elems), _ptr(labels)))
+    return nodes, elems, labels
+
+
+def refine_mesh(nodes, elems, labels=None):
+    """Uniform 1->4 refinement through the C ABI (1-based elements in and
+    out); returns (nodes, elems, labels or None)."""
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    elems = np.ascontiguousarray(elems, dtype=np.int32)
+    lab = None if labels is None else np.ascontiguousarray(labels, dtype=np.int32)
+    n2, m2 = ctypes.c_int(), ctypes.c_int()
+    args = (nodes.shape[0], _ptr(nodes), elems.shape[0], _ptr(elems), _ptr(lab))
+    check(lib().eb_mesh_refine(*args, ctypes.byref(n2), None, ctypes.byref(m2), None, None))
+    P2 = np.empty((n2.value, 3))
+    T2 = np.empty((m2.value, 3), dtype=np.int32)
+    L2 = None if lab is None else np.empty(m2.value, dtype=np.int32)
+    check(lib().eb_mesh_refine(*args, ctypes.byref(n2), _ptr(P2), ctypes.byref(m2), _ptr(T2), _ptr(L2)))
+    return P2, T2, L2
+
+
+class Batch:
+    """Applies of many meshes in one launch.
+
+    ``Batch(meshes, ncols)``: P0 single layer with ncols right-hand sides;
     ``apply_device(d_t, d_v, stream)`` takes lists of device pointers (one
-    [ncols][nelems] array per mesh).
+    [ncols][nelems] array per mesh). ``Batch(meshes, sl_dl=True)``: single
+    and double layer of one density pair per mesh in the same pass;
+    ``apply_sl_dl_device(d_t, d_u, d_v, d_q, stream)`` (t, v, q: [nelems],
+    u: [nnodes]) or ``apply_sl_dl(ts, us)`` with host arrays.
     """
 
-    def __init__(self, meshes, ncols: int = 1, precision="mixed"):
+    def __init__(self, meshes, ncols: int = 1, precision="mixed", sl_dl: bool = False):
         arr = (ctypes.c_void_p * len(meshes))(*[m.handle.value for m in meshes])
         h = ctypes.c_void_p()
-        check(lib().eb_batch_create(len(meshes), arr, int(ncols), precision_code(precision), ctypes.byref(h)))
+        if sl_dl:
+            check(lib().eb_batch_create_sl_dl(len(meshes), arr, precision_code(precision), ctypes.byref(h)))
+        else:
+            check(lib().eb_batch_create(len(meshes), arr, int(ncols), precision_code(precision), ctypes.byref(h)))
         self._h = h
         self.meshes = list(meshes)
         self.ncols = ncols
+        self.sl_dl = sl_dl
         q = ctypes.c_longlong()
         check(lib().eb_batch_info(h, ctypes.byref(q)))
         self.quad_pairs = q.value
@@ -231,6 +274,23 @@ class Batch:
         n = len(self.meshes)
         check(lib().eb_batch_apply(self._h, (ctypes.c_void_p * n)(*d_t), (ctypes.c_void_p * n)(*d_v),
                                    ctypes.c_void_p(stream or None)))
+
+    def apply_sl_dl_device(self, d_t, d_u, d_v, d_q, stream=0):
+        n = len(self.meshes)
+        arr = [(ctypes.c_void_p * n)(*x) for x in (d_t, d_u, d_v, d_q)]
+        check(lib().eb_batch_apply_sl_dl(self._h, *arr, ctypes.c_void_p(stream or None)))
+
+    def apply_sl_dl(self, ts, us):
+        """Host arrays in and out (through device copies made with torch)."""
+        import torch
+        dt = [torch.from_numpy(np.ascontiguousarray(t, dtype=np.float64)).cuda() for t in ts]
+        du = [torch.from_numpy(np.ascontiguousarray(u, dtype=np.float64)).cuda() for u in us]
+        dv = [torch.empty_like(t) for t in dt]
+        dq = [torch.empty_like(t) for t in dt]
+        torch.cuda.synchronize()
+        self.apply_sl_dl_device([x.data_ptr() for x in dt], [x.data_ptr() for x in du], [x.data_ptr() for x in dv],
+                                [x.data_ptr() for x in dq])
+        return [x.cpu().numpy() for x in dv], [x.cpu().numpy() for x in dq]
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

@@ -38,6 +38,8 @@ _SIGNATURES = {
     "eb_mesh_info": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "eb_mesh_finalize_bytes": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_mesh_near_field_bytes": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong),
+                                                ctypes.POINTER(ctypes.c_longlong)]),
     "eb_release_cached_memory": (ctypes.c_int, []),
     "eb_cached_memory_bytes": (ctypes.c_int, [ctypes.POINTER(ctypes.c_longlong)]),
     "eb_apply_sl_p0": (ctypes.c_int, [_dp, ctypes.c_int, _dp, _dp]),
@@ -71,6 +73,11 @@ _SIGNATURES = {
     "eb_batch_create": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp)]),
     "eb_batch_destroy": (ctypes.c_int, [_dp]),
     "eb_batch_apply": (ctypes.c_int, [_dp, _dp, _dp, _dp]),
+    "eb_read_surface_txt": (ctypes.c_int, [ctypes.c_char_p, _dp, _dp, _dp, _dp, _dp]),
+    "eb_read_netgen_vol": (ctypes.c_int, [ctypes.c_char_p, _dp, _dp, _dp, _dp, _dp]),
+    "eb_mesh_refine": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "eb_batch_create_sl_dl": (ctypes.c_int, [ctypes.c_int, _dp, ctypes.c_int, ctypes.POINTER(_dp)]),
+    "eb_batch_apply_sl_dl": (ctypes.c_int, [_dp, _dp, _dp, _dp, _dp, _dp]),
     "eb_batch_info": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong)]),
     "eb_server_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, _dp, ctypes.POINTER(_dp)]),
     "eb_server_destroy": (ctypes.c_int, [_dp]),

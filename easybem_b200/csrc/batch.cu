@@ -6,15 +6,22 @@
 
 namespace eb {
 
-int batch_entry_init(BatchEntry* e, Mesh* m)
+int batch_entry_init(BatchEntry* e, Mesh* m, bool with_dl)
 {
   const HostMesh& h = m->h;
   e->mesh = m;
-  EB_CHECK(e->rec.alloc((size_t)h.ne * h.Q * rec_slots(kBatchCols, false) * sizeof(dq)));
+  // record slots of the widest variant used: 4 SL charges, or SL + DL
+  static_assert(rec_slots(kBatchCols, 0) >= rec_slots(1, 1), "entry scratch sized for the SL+DL records");
+  EB_CHECK(e->rec.alloc((size_t)h.ne * h.Q * rec_slots(kBatchCols, 0) * sizeof(dq)));
   EB_CHECK(e->partial.alloc(sizeof(double) * (size_t)kBatchCols * m->plan.nsplit * h.nitems));
   EB_CHECK(e->tin.alloc(sizeof(double) * (size_t)kBatchCols * h.ne));
   EB_CHECK(e->vout.alloc(sizeof(double) * (size_t)kBatchCols * h.ne));
   EB_CHECK(memset_sync(e->tin.p, 0, e->tin.bytes));
+  if (with_dl) {
+    EB_CHECK(e->uin.alloc(sizeof(double) * (size_t)h.nv));
+    EB_CHECK(e->qout.alloc(sizeof(double) * (size_t)h.ne));
+    EB_CHECK(memset_sync(e->uin.p, 0, e->uin.bytes));
+  }
   return EB_OK;
 }
 
@@ -31,12 +38,14 @@ void Batch::reset_graph()
 
 int batch_width(int cols) { return cols <= 1 ? 1 : (cols <= 3 ? 3 : 4); }
 
-int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags)
+int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags, int nd)
 {
   reset_graph();
   entries_ = entries;
   fp32_ = fp32;
-  nsl_ = batch_width(nsl);
+  if (nd < 0 || nd > 1 || (nd == 1 && nsl > 1)) return set_error(EB_ERR_INVALID, "a DL batch takes 0 or 1 SL column");
+  nd_ = nd;
+  nsl_ = nd ? nsl : batch_width(nsl);
   nitems_ = grid_ = prep_blocks_ = fin_blocks_ = 0;
   quad_pairs_ = 0;
   if (entries.empty()) return EB_OK;
@@ -56,11 +65,13 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     if (h.Q != Q_) return set_error(EB_ERR_INVALID, "a batch needs one quadrature order for all meshes");
     // the mesh's plan may have changed (finer work split) since the entry was made
     EB_CHECK(be->partial.alloc(sizeof(double) * (size_t)kBatchCols * m->plan.nsplit * h.nitems));
-    desc[e] = mesh_far_desc(m, fp32, nsl_, false, be->rec.p, be->partial.as<double>());
+    if (nd_ && !be->uin.p) return set_error(EB_ERR_INVALID, "batch entry without DL columns");
+    desc[e] = mesh_far_desc(m, fp32, nsl_, nd_, be->rec.p, be->partial.as<double>());
     desc[e].active = d_flags ? d_flags + e : nullptr;
     src_tile = std::min(src_tile, desc[e].src_tile);
-    args[e] = mesh_apply_args(m, fp32, be->rec.p, be->partial.as<double>(), be->tin.as<double>(), h.ne, nullptr,
-                              be->vout.as<double>(), h.ne, nullptr);
+    args[e] = mesh_apply_args(m, fp32, be->rec.p, be->partial.as<double>(), nsl_ ? be->tin.as<double>() : nullptr,
+                              h.ne, nd_ ? be->uin.as<double>() : nullptr, nsl_ ? be->vout.as<double>() : nullptr,
+                              h.ne, nd_ ? be->qout.as<double>() : nullptr);
     args[e].active = d_flags ? d_flags + e : nullptr;
     poff[e + 1] = poff[e] + (int)(((long long)h.ne * h.Q + kPrepBlock - 1) / kPrepBlock);
     foff[e + 1] = foff[e] + (h.ne + kFinalizeRows - 1) / kFinalizeRows;
@@ -96,8 +107,8 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   EB_CHECK(copy_h2d(fin_off_.p, foff.data(), sizeof(int) * (n + 1)));
   EB_CHECK(counter_.alloc(sizeof(int)));
 
-  smem_ = far_smem_bytes(src_tile, Q_, rec_slots(nsl_, false), fp32);
-  int occ = far_occupancy(fp32, nsl_, false, K_, Q_, smem_);
+  smem_ = far_smem_bytes(src_tile, Q_, rec_slots(nsl_, nd_), fp32);
+  int occ = far_occupancy(fp32, nsl_, nd_, K_, Q_, smem_);
   if (occ < 1) occ = 1;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
@@ -114,11 +125,11 @@ int Batch::run(cudaStream_t st, int reserve_sms)
   const int n = (int)entries_.size();
   const int free_sms = std::max(1, nsm_ - std::max(0, reserve_sms));
   const int grid = reserve_sms > 0 ? std::min(grid_, free_sms * occ_) : grid_;
-  EB_CUDA(prep_launch_batch(fp32_, nsl_, false, args_.as<ApplyArgs>(), prep_off_.as<int>(), n, prep_blocks_, st));
+  EB_CUDA(prep_launch_batch(fp32_, nsl_, nd_, args_.as<ApplyArgs>(), prep_off_.as<int>(), n, prep_blocks_, st));
   EB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(int), st));
-  EB_CUDA(far_launch(fp32_, nsl_, false, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
+  EB_CUDA(far_launch(fp32_, nsl_, nd_, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
                      counter_.as<int>(), smem_, grid, st));
-  EB_CUDA(finalize_launch_batch(nsl_, false, args_.as<ApplyArgs>(), fin_off_.as<int>(), n, fin_blocks_, st));
+  EB_CUDA(finalize_launch_batch(nsl_, nd_, args_.as<ApplyArgs>(), fin_off_.as<int>(), n, fin_blocks_, st));
   return EB_OK;
 }
 
@@ -163,9 +174,39 @@ struct eb_batch_s {
   eb::DevBuf flags;
   cudaStream_t stream = nullptr;
   int ncols = 1;
+  bool sl_dl = false;  // made by eb_batch_create_sl_dl
 };
 
 using eb::set_error;
+
+static int batch_create(int nmesh, const eb_mesh* meshes, int ncols, int nd, int precision, eb_batch* out)
+{
+  if (precision != EB_PREC_FP64 && precision != EB_PREC_MIXED)
+    return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
+  auto b = std::make_unique<eb_batch_s>();
+  b->ncols = ncols;
+  b->sl_dl = nd > 0;
+  std::vector<eb::BatchEntry*> ents;
+  int dev = -1;
+  for (int i = 0; i < nmesh; i++) {
+    if (!meshes[i]) return set_error(EB_ERR_INVALID, "null mesh");
+    eb::Mesh* m = eb_mesh_internal(meshes[i]);
+    if (dev >= 0 && m->device != dev) return set_error(EB_ERR_INVALID, "a batch needs all meshes on one device");
+    dev = m->device;
+    EB_CUDA(cudaSetDevice(dev));
+    auto e = std::make_unique<eb::BatchEntry>();
+    EB_CHECK(eb::batch_entry_init(e.get(), m, nd > 0));
+    ents.push_back(e.get());
+    b->entries.push_back(std::move(e));
+  }
+  EB_CHECK(b->flags.alloc(sizeof(int) * nmesh));
+  std::vector<int> ones(nmesh, 1);
+  EB_CHECK(eb::copy_h2d(b->flags.p, ones.data(), sizeof(int) * nmesh));
+  EB_CHECK(b->batch.build(ents, precision == EB_PREC_MIXED, ncols, b->flags.as<int>(), nd));
+  EB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  *out = b.release();
+  return EB_OK;
+}
 
 extern "C" {
 
@@ -173,25 +214,13 @@ int eb_batch_create(int nmesh, const eb_mesh* meshes, int ncols, int precision, 
 {
   if (!out || nmesh < 1 || !meshes || ncols < 1 || ncols > eb::kBatchCols)
     return set_error(EB_ERR_INVALID, "need >= 1 mesh and 1..4 columns");
-  if (precision != EB_PREC_FP64 && precision != EB_PREC_MIXED)
-    return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
-  auto b = std::make_unique<eb_batch_s>();
-  b->ncols = ncols;
-  std::vector<eb::BatchEntry*> ents;
-  for (int i = 0; i < nmesh; i++) {
-    if (!meshes[i]) return set_error(EB_ERR_INVALID, "null mesh");
-    auto e = std::make_unique<eb::BatchEntry>();
-    EB_CHECK(eb::batch_entry_init(e.get(), eb_mesh_internal(meshes[i])));
-    ents.push_back(e.get());
-    b->entries.push_back(std::move(e));
-  }
-  EB_CHECK(b->flags.alloc(sizeof(int) * nmesh));
-  std::vector<int> ones(nmesh, 1);
-  EB_CHECK(eb::copy_h2d(b->flags.p, ones.data(), sizeof(int) * nmesh));
-  EB_CHECK(b->batch.build(ents, precision == EB_PREC_MIXED, ncols, b->flags.as<int>()));
-  EB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  *out = b.release();
-  return EB_OK;
+  return batch_create(nmesh, meshes, ncols, 0, precision, out);
+}
+
+int eb_batch_create_sl_dl(int nmesh, const eb_mesh* meshes, int precision, eb_batch* out)
+{
+  if (!out || nmesh < 1 || !meshes) return set_error(EB_ERR_INVALID, "need >= 1 mesh");
+  return batch_create(nmesh, meshes, 1, 1, precision, out);
 }
 
 int eb_batch_destroy(eb_batch b)
@@ -205,9 +234,32 @@ int eb_batch_destroy(eb_batch b)
   return EB_OK;
 }
 
+int eb_batch_apply_sl_dl(eb_batch b, const double* const* d_t, const double* const* d_u, double* const* d_v,
+                         double* const* d_q, void* stream)
+{
+  if (!b || !d_t || !d_u || !d_v || !d_q) return set_error(EB_ERR_INVALID, "null argument");
+  if (!b->sl_dl) return set_error(EB_ERR_INVALID, "batch made by eb_batch_create: use eb_batch_apply");
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  for (size_t i = 0; i < b->entries.size(); i++) {
+    const eb::BatchEntry& e = *b->entries[i];
+    if (!d_t[i] || !d_u[i] || !d_v[i] || !d_q[i]) return set_error(EB_ERR_INVALID, "null vector");
+    EB_CUDA(cudaMemcpyAsync(e.tin.p, d_t[i], sizeof(double) * e.mesh->h.ne, cudaMemcpyDeviceToDevice, st));
+    EB_CUDA(cudaMemcpyAsync(e.uin.p, d_u[i], sizeof(double) * e.mesh->h.nv, cudaMemcpyDeviceToDevice, st));
+  }
+  EB_CHECK(b->batch.run_graph(st));
+  for (size_t i = 0; i < b->entries.size(); i++) {
+    const eb::BatchEntry& e = *b->entries[i];
+    EB_CUDA(cudaMemcpyAsync(d_v[i], e.vout.p, sizeof(double) * e.mesh->h.ne, cudaMemcpyDeviceToDevice, st));
+    EB_CUDA(cudaMemcpyAsync(d_q[i], e.qout.p, sizeof(double) * e.mesh->h.ne, cudaMemcpyDeviceToDevice, st));
+  }
+  if (!stream) EB_CUDA(cudaStreamSynchronize(st));
+  return EB_OK;
+}
+
 int eb_batch_apply(eb_batch b, const double* const* d_t, double* const* d_v, void* stream)
 {
   if (!b || !d_t || !d_v) return set_error(EB_ERR_INVALID, "null argument");
+  if (b->sl_dl) return set_error(EB_ERR_INVALID, "batch made by eb_batch_create_sl_dl: use eb_batch_apply_sl_dl");
   cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
   for (size_t i = 0; i < b->entries.size(); i++) {
     const size_t bytes = sizeof(double) * (size_t)b->ncols * b->entries[i]->mesh->h.ne;

@@ -26,6 +26,7 @@ struct BatchEntry {
   Mesh* mesh = nullptr;
   DevBuf rec, partial;  // apply scratch
   DevBuf tin, vout;     // kBatchCols columns of nelems each (inputs / outputs)
+  DevBuf uin, qout;     // DL density [nnodes] and DL output [nelems] (batches with a DL column)
   int index = -1;       // position in the current batch
 };
 
@@ -34,8 +35,9 @@ class Batch {
   // Builds the launch tables for `entries` (all meshes must share the
   // quadrature order). fp32 selects the mixed-precision far field.
   // nsl: right-hand sides computed per entry (1, 3 or 4; columns beyond an
-  // entry's systems carry zeros).
-  int build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags);
+  // entry's systems carry zeros). nd = 1 adds the double layer (uin -> qout)
+  // in the same pass, with nsl 0 or 1 (the fused SL+DL variant).
+  int build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags, int nd = 0);
   // One apply of all entries whose flag is set (inputs tin, outputs vout).
   // reserve_sms > 0 sizes the persistent far-field grid to leave that many
   // SMs free for kernels of other streams (the far kernel holds every SM it
@@ -54,6 +56,7 @@ class Batch {
   std::vector<BatchEntry*> entries_;
   bool fp32_ = true;
   int nsl_ = kBatchCols;
+  int nd_ = 0;
   DevBuf desc_, items_, args_, prep_off_, fin_off_, counter_;
   int nitems_ = 0, grid_ = 0, occ_ = 1, nsm_ = 148, prep_blocks_ = 0, fin_blocks_ = 0, K_ = 0, Q_ = 0;
   size_t smem_ = 0;
@@ -66,7 +69,8 @@ class Batch {
 
 // Far-field variant width (SL charges) for entries using up to `cols` columns.
 int batch_width(int cols);
-// Allocates an entry's scratch and columns for mesh m.
-int batch_entry_init(BatchEntry* e, Mesh* m);
+// Allocates an entry's scratch and columns for mesh m (with_dl: also the DL
+// density and output).
+int batch_entry_init(BatchEntry* e, Mesh* m, bool with_dl = false);
 
 }  // namespace eb

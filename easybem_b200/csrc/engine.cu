@@ -767,6 +767,20 @@ int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes)
   return EB_OK;
 }
 
+int eb_mesh_near_field_bytes(eb_mesh mesh, long long* spmv_bytes, long long* fold_bytes)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null argument");
+  const eb::HostMesh& h = mesh->m->h;
+  const long long ne = h.ne, sl = (long long)h.sl_col.size(), dl = (long long)h.dl_col.size();
+  // the SL and DL near-field SpMVs: row pointers, per entry column + value +
+  // gathered density, one FP64 output per row and operator
+  if (spmv_bytes) *spmv_bytes = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8) + 2 * 8 * ne;
+  // the fold of the far-field partial sums: both outputs' partial slots, the
+  // row's normal/area record and its permutation entry
+  if (fold_bytes) *fold_bytes = 2 * 8LL * mesh->m->plan.nsplit * h.nitems + 8 * ne + 4 * ne;
+  return EB_OK;
+}
+
 int eb_apply_sl_dl_device(eb_mesh mesh, int precision, const double* d_t, const double* d_u, double* d_v,
                           double* d_q, void* stream)
 {

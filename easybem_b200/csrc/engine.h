@@ -118,7 +118,7 @@ struct Mesh {
   // hypersingular: curl coefficients, vertex -> (triangle, local) lists, work vectors
   DevBuf curl9, vtri_ptr, vtri_list, elems0, hs_x, hs_w;
   // potential evaluation: per-chunk partial sums and host-call staging
-  DevBuf pot_partial, io_pts, io_pot;
+  DevBuf pot_partial, io_pts, io_pot, pot_rec64;
   int nitems_work = 0;
   FarPlan plan;
   // one immutable device descriptor and launch shape per far-field variant

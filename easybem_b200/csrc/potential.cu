@@ -10,6 +10,13 @@
 // the SL+DL apply prepares (charges w_b J_j t_j and strengths w_b J_j u_h);
 // (x - y).n_j is the signed distance of x from the plane of triangle j. FP32
 // evaluates cell-relative coordinates with per-cell two-sum accumulation.
+//
+// In FP32 the cell-relative coordinates round to ~6e-8 of the cell radius R;
+// for a point closer to a cell than about 2R that error is no longer small
+// next to the distances, and near the surface the terms of neighbouring
+// triangles cancel on top of it. The FP32 kernel therefore sums every cell
+// whose centre lies within kPotNear * R of a point in FP64 (from FP64
+// records; a few cells per point near the surface, none away from it).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,6 +29,30 @@
 namespace eb {
 
 constexpr int kPotThreads = 128;
+constexpr double kPotNear = 2.5;  // cells within this many radii of a point are summed in FP64
+
+// One cell's contribution to u(x) in FP64 from FP64 records ([ne*Q][2] dq)
+// and planes, (xs, ys, zs) = x relative to the cell centre.
+__device__ __noinline__ double pot_cell_fp64(double xs, double ys, double zs, const dq* __restrict__ rec64,
+                                             const dq* __restrict__ plane64, int s0, int s1, int Q)
+{
+  double part = 0.0;
+  for (int s = s0; s < s1; ++s) {
+    const dq pn = plane64[s];
+    const double d = xs * pn.x + (ys * pn.y + (zs * pn.z - pn.w));
+    double sl = 0.0, acc = 0.0;
+    const dq* r = rec64 + (size_t)s * Q * 2;
+    for (int b = 0; b < Q; ++b) {
+      const dq p0 = r[2 * b], p1 = r[2 * b + 1];
+      const double dx = xs + 0.5 * p0.x, dy = ys + 0.5 * p0.y, dz = zs + 0.5 * p0.z;
+      const double inv = rsqrt(dx * dx + dy * dy + dz * dz);
+      sl += p1.y * inv;
+      acc += (inv * inv) * (p1.x * inv);
+    }
+    part += sl - d * acc;
+  }
+  return part;
+}
 
 __device__ __forceinline__ void pot_two_sum(float& s, float& e, float x)
 {
@@ -116,6 +147,8 @@ __global__ void __launch_bounds__(kPotThreads) potential_x2_kernel(int npts, con
                                                                    const float4* __restrict__ rec,
                                                                    const float4* __restrict__ plane,
                                                                    const dq* __restrict__ ccent,
+                                                                   const dq* __restrict__ rec64,
+                                                                   const dq* __restrict__ plane64,
                                                                    double* __restrict__ partial)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -131,6 +164,7 @@ __global__ void __launch_bounds__(kPotThreads) potential_x2_kernel(int npts, con
   const int sb = c0 * kCell, se = min(ne, c1 * kCell);
   const float2 half2 = make_float2(0.5f, 0.5f);
   float hi[2] = {0.f, 0.f}, lo[2] = {0.f, 0.f};
+  double near[2] = {0.0, 0.0};  // FP64 sums of the cells close to each point
   for (int t0 = sb; t0 < se; t0 += kTS) {
     const int ns = min(kTS, se - t0);
     for (int k = threadIdx.x; k < ns * Q * 2; k += kPotThreads) s_rec[k] = rec[(size_t)t0 * Q * 2 + k];
@@ -164,15 +198,22 @@ __global__ void __launch_bounds__(kPotThreads) potential_x2_kernel(int npts, con
           }
           part = __fadd2_rn(part, __ffma2_rn(make_float2(-d.x, -d.y), acc, sl));
         }
-        pot_two_sum(hi[0], lo[0], part.x);
-        pot_two_sum(hi[1], lo[1], part.y);
+        const double rn2 = kPotNear * kPotNear * cc.w * cc.w;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const double ex = px[k] - cc.x, ey = py[k] - cc.y, ez = pz[k] - cc.z;
+          const bool close = (k == 0 || a1) && ex * ex + ey * ey + ez * ez < rn2;
+          if (close) near[k] += pot_cell_fp64(ex, ey, ez, rec64, plane64, t0 + g0, t0 + g1, Q);
+          const float pk = close ? 0.f : (k == 0 ? part.x : part.y);
+          pot_two_sum(hi[k], lo[k], pk);
+        }
         g0 = g1;
       }
     }
     __syncthreads();
   }
-  if (a0) partial[(size_t)blockIdx.y * npts + i0] = (double)hi[0] + (double)lo[0];
-  if (a1) partial[(size_t)blockIdx.y * npts + i1] = (double)hi[1] + (double)lo[1];
+  if (a0) partial[(size_t)blockIdx.y * npts + i0] = (double)hi[0] + (double)lo[0] + near[0];
+  if (a1) partial[(size_t)blockIdx.y * npts + i1] = (double)hi[1] + (double)lo[1] + near[1];
 }
 
 __global__ void potential_reduce_kernel(int npts, int nchunk, const double* __restrict__ partial,
@@ -201,6 +242,11 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
   }
   const ApplyArgs A = mesh_apply_args(m, fp32, m->rec.p, nullptr, d_t, h.ne, d_u, nullptr, h.ne, nullptr);
   EB_CUDA(prep_launch(fp32, 1, true, A, st));
+  if (fp32) {  // FP64 records for the cells close to a point
+    EB_CHECK(m->pot_rec64.alloc((size_t)h.ne * h.Q * rec_slots(1, 1) * sizeof(dq)));
+    const ApplyArgs A64 = mesh_apply_args(m, false, m->pot_rec64.p, nullptr, d_t, h.ne, d_u, nullptr, h.ne, nullptr);
+    EB_CUDA(prep_launch(false, 1, true, A64, st));
+  }
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
   const int per_block = fp32 ? 2 * kPotThreads : kPotThreads;  // the FP32 kernel takes two points per thread
@@ -215,7 +261,8 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
     auto k = potential_x2_kernel;
     if (smem > 32 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, m->rec.as<float4>(),
-                                       m->splane32.as<float4>(), m->ccent.as<dq>(), m->pot_partial.as<double>());
+                                       m->splane32.as<float4>(), m->ccent.as<dq>(), m->pot_rec64.as<dq>(),
+                                       m->splane64.as<dq>(), m->pot_partial.as<double>());
   } else {
     auto k = potential_kernel<double>;
     if (smem > 32 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

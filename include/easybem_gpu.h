@@ -65,6 +65,11 @@ int eb_cached_memory_bytes(long long* bytes);
  * the outputs): the numerator of its HBM roofline. No counterpart in the
  * reference. */
 int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes);
+/* The same bytes split into the near-field SpMV of both operators (CSR row
+ * pointers, columns and values, gathered densities, outputs) and the fold of
+ * the far-field partial sums that the same launch performs. No counterpart
+ * in the reference. */
+int eb_mesh_near_field_bytes(eb_mesh mesh, long long* spmv_bytes, long long* fold_bytes);
 
 /* v = V t, the P0 single layer (Galerkin, kernel 1/(4 pi |x-y|)); t and v
  * have nelems entries, host memory. Replaces applyGPULaplace3d1Layer(t, v, 0)
@@ -135,6 +140,17 @@ int eb_batch_destroy(eb_batch batch);
 int eb_batch_apply(eb_batch batch, const double* const* d_t, double* const* d_v, void* stream);
 /* Regular quadrature-point pairs one batched apply evaluates (per column set). */
 int eb_batch_info(eb_batch batch, long long* quad_pairs);
+/* Batched single and double layer: v_i = V_i t_i and q_i = K_i u_i for every
+ * mesh i in one persistent far-field pass (the fused variant of
+ * eb_apply_sl_dl; each quadrature-pair distance serves both operators). d_t,
+ * d_v, d_q hold device arrays of nelems_i entries, d_u of nnodes_i. Stream
+ * semantics as eb_batch_apply; eb_batch_info counts each pair once. No
+ * counterpart in the reference (one mesh per process, applyGPULaplace3d1Layer
+ * and applyGPULaplace3d2Layer as separate passes, src/BEM3dLaplaceGPU.cu:
+ * 985-1551). */
+int eb_batch_create_sl_dl(int nmesh, const eb_mesh* meshes, int precision, eb_batch* out);
+int eb_batch_apply_sl_dl(eb_batch batch, const double* const* d_t, const double* const* d_u,
+                         double* const* d_v, double* const* d_q, void* stream);
 
 /* ---- Solves: V x = b (P0 single layer) by GMRES with iterative refinement.
  * No counterpart in the reference (its drivers call SciPy CG on FP32 GPU
@@ -250,6 +266,27 @@ int eb_dirichlet_rhs_prec(eb_mesh mesh, int precision, int nrhs, const double* g
  * 284-305, 1045-1070. Arrays must hold 64 and 79 entries. */
 int eb_quadrature(int order, int* nline, double* lx, double* lw, int* ntri, double* tx, double* ty,
                   double* tw);
+
+/* ---- Mesh ingestion (host only, no GPU needed). Readers of the two surface
+ * formats the reference's drivers load: easybem's plain-text surface
+ * (python/examples/surface3dMesh.py:51-83 load3dSurface: dimension, vertices
+ * per element, vertex list, triangle list, then "index label" lines) and the
+ * surface triangles of a Netgen .vol file (:86-146 load3dSurfaceFromNetgen:
+ * sections "points" and "surfaceelementsgi", label = surface number).
+ * nodes [nnodes][3], elems [nelems][3] 1-based, labels [nelems]; with null
+ * arrays only the counts are written (call once for sizes, once to fill). */
+int eb_read_surface_txt(const char* path, int* nnodes, double* nodes, int* nelems, int* elems, int* labels);
+int eb_read_netgen_vol(const char* path, int* nnodes, double* nodes, int* nelems, int* elems, int* labels);
+/* Uniform 1->4 refinement (:149-221 refineMesh): one midpoint per unique
+ * edge, numbered after the old vertices in lexicographic order of the
+ * edge's (smaller, larger) vertex pair; children of triangle k at k, m + k,
+ * 2m + k, 3m + k (m = nelems): (v0, m01, m20), (m01, v1, m12),
+ * (m20, m12, v2), (m01, m12, m20). Child labels are their parent's (the
+ * reference repeats each label four times in a row instead, so its labels
+ * do not follow its own child order). With null output arrays only the
+ * counts are written. labels and labels_out may be null. */
+int eb_mesh_refine(int nnodes, const double* nodes, int nelems, const int* elems, const int* labels,
+                   int* nnodes_out, double* nodes_out, int* nelems_out, int* elems_out, int* labels_out);
 
 /* Roofline calibration: sustained FP32 FFMA throughput of the current GPU in
  * TFLOP/s (FMA = 2 flops), from a register-only FMA-chain kernel. No
