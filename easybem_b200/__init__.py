@@ -163,6 +163,16 @@ class Mesh:
         check(lib().eb_apply_near_precond(self._h, _ptr(x), _ptr(y)))
         return y
 
+    def set_far_engine(self, engine: str = "tensor"):
+        """Far-field engine of the fused mixed SL+DL apply: "tensor" (tcgen05
+        GEMMs for the pair distances) or "cuda" (FP32 pipes only)."""
+        check(lib().eb_mesh_set_far_engine(self._h, {"cuda": 0, "tensor": 1}[engine]))
+
+    def far_engine(self, precision="mixed"):
+        e = ctypes.c_int()
+        check(lib().eb_mesh_get_far_engine(self._h, precision_code(precision), ctypes.byref(e)))
+        return "tensor" if e.value == 1 else "cuda"
+
     def set_profiling(self, on: bool = True):
         check(lib().eb_set_profiling(self._h, 1 if on else 0))
 

@@ -1,6 +1,7 @@
 // Device-resident mesh, FP64 Sauter-Schwab near field and the apply pipeline
 // (prep -> far field -> finalize), plus the C ABI of include/easybem_gpu.h.
 #include "engine.h"
+#include "farfield_tc.h"
 
 #include <algorithm>
 #include <chrono>
@@ -521,6 +522,8 @@ int mesh_set_plan(Mesh* m, int items_per_sm, int tile)
     v.desc.release();
     v.grid = 0;
   }
+  m->tc_var.desc.release();
+  m->tc_var.grid = 0;
   m->rec.release();
   m->partial.release();
   return build_items(m);
@@ -622,6 +625,57 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
   return desc;
 }
 
+bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd)
+{
+  return m->plan.engine == 1 && fp32 && nsl == 1 && nd == 1 && m->h.Q == kTcRule && m->h.K == kTcRule;
+}
+
+// The tensor-core far field: static operands once per mesh, then per apply
+// the DL operand and charges from the records, the persistent kernel.
+static int tc_far_apply(Mesh* m, cudaStream_t st)
+{
+  const HostMesh& h = m->h;
+  if (!m->tc_static_ready) {
+    EB_CHECK(m->tc_bd2.alloc(far_tc_operand_bytes(h.ncells)));
+    EB_CHECK(m->tc_be.alloc(far_tc_operand_bytes(h.ncells)));
+    EB_CHECK(m->tc_charge.alloc(far_tc_charge_bytes(h.ncells)));
+    EB_CHECK(m->tc_err.alloc(sizeof(int)));
+    EB_CHECK(memset_sync(m->tc_err.p, 0, sizeof(int)));
+    EB_CUDA(far_tc_prep_static(h.ne, h.ncells, m->pos32.as<float4>(), m->tc_bd2.as<float4>(), st));
+    m->tc_static_ready = true;
+  }
+  if (!m->tc_var.desc.p) {  // (re)built after a plan change: scratch pointers and split
+    FarMeshDesc desc = mesh_far_desc(m, true, 1, 1, m->rec.p, m->partial.as<double>());
+    desc.tc_bd2 = m->tc_bd2.as<float4>();
+    desc.tc_be = m->tc_be.as<float4>();
+    desc.tc_charge = m->tc_charge.as<float>();
+    EB_CHECK(m->tc_var.desc.alloc(sizeof(FarMeshDesc)));
+    EB_CHECK(copy_h2d(m->tc_var.desc.p, &desc, sizeof desc));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    m->tc_var.grid = std::min(nsm, std::max(1, m->nitems_work));
+  }
+  EB_CUDA(far_tc_prep_dl(h.ne, h.ncells, m->rec.as<float4>(), m->splane32.as<float4>(), m->tc_be.as<float4>(),
+                         m->tc_charge.as<float>(), st));
+  EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
+  if (m->profile) EB_CUDA(cudaEventRecord(m->ev0, st));
+  EB_CUDA(far_tc_launch(m->tc_var.desc.as<FarMeshDesc>(), m->items.as<WorkItem>(), m->nitems_work,
+                        m->counter.as<int>(), m->tc_err.as<int>(), m->tc_var.grid, st));
+  m->plan.grid = m->tc_var.grid;
+  m->tc_used = true;
+  return EB_OK;
+}
+
+int mesh_check_far_error(Mesh* m)
+{
+  if (!m->tc_used || !m->tc_err.p) return EB_OK;
+  int flag = 0;
+  EB_CHECK(copy_d2h(&flag, m->tc_err.p, sizeof(int)));
+  if (!flag) return EB_OK;
+  EB_CHECK(memset_sync(m->tc_err.p, 0, sizeof(int)));
+  return set_error(EB_ERR_TIMEOUT, "tensor-core far field: a bounded wait for the tensor cores ran out");
+}
+
 int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const double* d_u, double* d_v,
                double* d_q, cudaStream_t st)
 {
@@ -655,18 +709,21 @@ int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const
   }
   const ApplyArgs A = mesh_apply_args(m, fp32, m->rec.p, m->partial.as<double>(), d_t, h.ne, d_u, d_v, h.ne, d_q);
   EB_CUDA(prep_launch(fp32, nsl, nd, A, st));
-  EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
-  if (m->profile) {
-    if (!m->ev0) {
-      EB_CUDA(cudaEventCreate(&m->ev0));
-      EB_CUDA(cudaEventCreate(&m->ev1));
-      EB_CUDA(cudaEventCreate(&m->ev2));
-    }
-    EB_CUDA(cudaEventRecord(m->ev0, st));
+  if (m->profile && !m->ev0) {
+    EB_CUDA(cudaEventCreate(&m->ev0));
+    EB_CUDA(cudaEventCreate(&m->ev1));
+    EB_CUDA(cudaEventCreate(&m->ev2));
   }
-  EB_CUDA(far_launch(fp32, nsl, nd, h.K, h.Q, var.desc.as<FarMeshDesc>(), m->items.as<WorkItem>(), m->nitems_work,
-                     m->counter.as<int>(), var.smem, var.grid, st));
-  m->plan.grid = var.grid;
+  if (tc_eligible(m, fp32, nsl, nd)) {
+    EB_CHECK(tc_far_apply(m, st));
+  } else {
+    EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
+    if (m->profile) EB_CUDA(cudaEventRecord(m->ev0, st));
+    EB_CUDA(far_launch(fp32, nsl, nd, h.K, h.Q, var.desc.as<FarMeshDesc>(), m->items.as<WorkItem>(), m->nitems_work,
+                       m->counter.as<int>(), var.smem, var.grid, st));
+    m->plan.grid = var.grid;
+    m->tc_used = false;
+  }
   m->plan.smem = var.smem;
   m->plan.src_tile = var.src_tile;
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev1, st));
@@ -817,7 +874,7 @@ static int host_apply(eb_mesh mesh, int precision, const double* t, const double
   if (sl) EB_CUDA(cudaMemcpyAsync(v, m->io_v.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
   if (dl) EB_CUDA(cudaMemcpyAsync(q, m->io_q.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st));
   EB_CUDA(cudaStreamSynchronize(st));
-  return EB_OK;
+  return eb::mesh_check_far_error(m);
 }
 
 int eb_apply_sl_p0(eb_mesh mesh, int precision, const double* t, double* v)
@@ -928,6 +985,22 @@ int eb_evaluate_potential(eb_mesh mesh, int precision, int npts, const double* p
                                        m->io_u.as<double>(), m->io_pot.as<double>(), st));
   EB_CUDA(cudaMemcpyAsync(out, m->io_pot.p, sizeof(double) * (size_t)npts, cudaMemcpyDeviceToHost, st));
   EB_CUDA(cudaStreamSynchronize(st));
+  return EB_OK;
+}
+
+int eb_mesh_set_far_engine(eb_mesh mesh, int engine)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  if (engine != EB_FAR_CUDA_CORES && engine != EB_FAR_TENSOR_CORES)
+    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES or EB_FAR_TENSOR_CORES");
+  mesh->m->plan.engine = engine;
+  return EB_OK;
+}
+
+int eb_mesh_get_far_engine(eb_mesh mesh, int precision, int* engine)
+{
+  if (!mesh || !engine) return set_error(EB_ERR_INVALID, "null argument");
+  *engine = eb::tc_eligible(mesh->m, precision == EB_PREC_MIXED, 1, 1) ? EB_FAR_TENSOR_CORES : EB_FAR_CUDA_CORES;
   return EB_OK;
 }
 

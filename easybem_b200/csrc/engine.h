@@ -88,6 +88,7 @@ struct DevBuf {
 
 // Launch plan of the far field for one mesh (tile shape and work split).
 struct FarPlan {
+  int engine = 0;         // 0: CUDA-core far kernel; 1: tensor-core kernel where the variant has one
   int items_per_sm = 32;  // work items per SM the source ranges are cut into (load balance)
   int tile = 0;           // source triangles per shared-memory tile (0: the variant's default)
   int src_tile = kTS;     // tile of the last launch
@@ -130,6 +131,12 @@ struct Mesh {
     int src_tile = 0;
   };
   Variant variants[128];
+  // tensor-core far field (fused FP32 SL+DL, 7-point rule): source operands
+  // per cell, SL charges, a bounded-wait error flag and its descriptor
+  DevBuf tc_bd2, tc_be, tc_charge, tc_err;
+  Variant tc_var;
+  bool tc_static_ready = false;
+  bool tc_used = false;  // the last apply ran the tensor-core kernel
   // host seconds of mesh creation: topology and pairs, static tables, near
   // field, and within the tables their device allocation and copy
   double setup_s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -149,6 +156,12 @@ ApplyArgs mesh_apply_args(const Mesh* m, bool fp32, void* rec, const double* par
 int src_tile_for(int Q, bool fp32, int nsl, int nd);
 // Far-field descriptor of mesh m for the given scratch.
 FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, double* partial);
+// True when mesh m applies the fused FP32 SL+DL far field with the
+// tensor-core kernel (engine 1, 7-point rule).
+bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd);
+// EB_ERR_TIMEOUT (and the flag cleared) if the last tensor-core launch on m
+// gave up a bounded wait; EB_OK otherwise. The stream must be synchronised.
+int mesh_check_far_error(Mesh* m);
 // Device-pointer apply: t has nsl columns (stride ne), v likewise; u has nd
 // DL columns (stride nnodes), q likewise (stride ne).
 int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const double* d_u, double* d_v,

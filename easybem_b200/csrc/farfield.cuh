@@ -91,6 +91,10 @@ struct FarMeshDesc {
   const dq* ttile;      // [ntiles]: target-tile centre and bounding radius (FP64)
   double* partial;      // [nout][nsplit][nitems]
   const int* active;    // optional: skip this mesh's work while *active == 0
+  // tensor-core kernel only: source operands per cell (UMMA layout) and charges
+  const float4* tc_bd2;
+  const float4* tc_be;
+  const float* tc_charge;
   int nitems, ne, Q, nsplit, src_tile;
 };
 

@@ -1,0 +1,30 @@
+// Tensor-core far field of the fused FP32 SL+DL apply (farfield_tc.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "farfield.cuh"
+
+namespace eb {
+
+constexpr int kTcChunk = 112;  // source points per MMA (half a cell: 16 triangles x 7 points)
+constexpr int kTcRule = 7;     // triangle-rule points the kernel is built for (quadrature index 4)
+
+// Bytes of the per-mesh source operands: one 14,336-byte block (224 rows x
+// 64 bytes) per cell for the distance GEMM, the same for the DL GEMM, and one
+// float charge per padded source point.
+inline size_t far_tc_operand_bytes(int ncells) { return (size_t)ncells * kCell * kTcRule * 64; }
+inline size_t far_tc_charge_bytes(int ncells) { return (size_t)ncells * kCell * kTcRule * 4; }
+
+// Once per mesh: the distance-GEMM source operand from the FP32 positions.
+cudaError_t far_tc_prep_static(int ne, int ncells, const float4* pos32, float4* bd2, cudaStream_t st);
+// Per apply, after the record preparation of the fused FP32 variant: the
+// DL-GEMM source operand and the SL charges.
+cudaError_t far_tc_prep_dl(int ne, int ncells, const float4* rec, const float4* splane32, float4* be, float* charges,
+                           cudaStream_t st);
+// The persistent kernel (grid = SM count); *d_error becomes 1 if a bounded
+// wait ran out.
+cudaError_t far_tc_launch(const FarMeshDesc* d_meshes, const WorkItem* d_items, int nitems, int* d_counter,
+                          int* d_error, int grid, cudaStream_t st);
+
+}  // namespace eb

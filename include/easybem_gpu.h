@@ -316,6 +316,20 @@ int eb_last_kernel_ms(eb_mesh mesh, double* far_ms, double* finalize_ms);
 int eb_mesh_set_plan(eb_mesh mesh, int items_per_sm, int src_tile);
 int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit, int* work_items);
 
+/* Far-field engine of a mesh's fused FP32 SL+DL apply (EB_PREC_MIXED, both
+ * operators, 7-point triangle rule = quadrature index 4):
+ * EB_FAR_CUDA_CORES evaluates every quadrature pair on the FP32 pipes;
+ * EB_FAR_TENSOR_CORES computes |x - y|^2 and the double-layer numerator
+ * s (x - y).n of well-separated cells as split-TF32 GEMMs on the tensor
+ * cores (tcgen05) and keeps the reciprocal square root and the sums on the
+ * CUDA cores. Other variants always use the CUDA cores; get reports the
+ * engine an apply in `precision` with both operators would use. No counterpart
+ * in the reference. */
+#define EB_FAR_CUDA_CORES 0
+#define EB_FAR_TENSOR_CORES 1
+int eb_mesh_set_far_engine(eb_mesh mesh, int engine);
+int eb_mesh_get_far_engine(eb_mesh mesh, int precision, int* engine);
+
 /* Times candidate plans (items_per_sm in {4,8,...,512} x source tile in
  * {default, 32, 16}) on this mesh with CUDA events, median of `reps` applies
  * each; operators: 1 = SL, 2 = DL, 3 = SL+DL. Keeps the fastest on the mesh
