@@ -163,6 +163,12 @@ class Mesh:
         check(lib().eb_apply_near_precond(self._h, _ptr(x), _ptr(y)))
         return y
 
+    def cell_pairs(self):
+        """(triangle pairs in well-separated source cells, in the other cells)."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().eb_mesh_cell_pairs(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def set_far_engine(self, engine: str = "tensor"):
         """Far-field engine of the fused mixed SL+DL apply: "tensor" (tcgen05
         GEMMs for the pair distances) or "cuda" (FP32 pipes only)."""

@@ -388,6 +388,21 @@ static int build_static(Mesh* m)
       }
     ttile[t] = dq{c.x, c.y, c.z, std::sqrt(r2) * (1.0 + 1e-12)};
   }
+  // how the tile x cell blocks split under the kernels' separation test
+  {
+    long long fc = 0, nc = 0;
+    for (int t = 0; t < ntt; t++) {
+      const long long nt = std::min(h.nitems, (t + 1) * kTT) - t * kTT;  // target items of the tile
+      for (int c = 0; c < h.ncells; c++) {
+        const long long ns = std::min(ne, (c + 1) * kCell) - c * kCell;
+        const double dx = ccent[c].x - ttile[t].x, dy = ccent[c].y - ttile[t].y, dz = ccent[c].z - ttile[t].z;
+        const double rr = kFarRatio * (ccent[c].w + ttile[t].w);
+        (dx * dx + dy * dy + dz * dz > rr * rr ? fc : nc) += nt * ns;
+      }
+    }
+    h.far_cell_tri_pairs = fc;
+    h.near_cell_tri_pairs = nc;
+  }
   // one allocation and one copy for all static tables (a mesh set-up that
   // runs beside other GPU work pays the per-call latency of the runtime once)
   struct Part {
@@ -821,6 +836,14 @@ int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes)
   long long b = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8);
   b += 2 * 8LL * mesh->m->plan.nsplit * h.nitems + 2 * 8 * ne + 8 * ne /* trin */ + 4 * ne /* iperm */;
   *bytes = b;
+  return EB_OK;
+}
+
+int eb_mesh_cell_pairs(eb_mesh mesh, long long* far_cell_tri_pairs, long long* near_cell_tri_pairs)
+{
+  if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
+  if (far_cell_tri_pairs) *far_cell_tri_pairs = mesh->m->h.far_cell_tri_pairs;
+  if (near_cell_tri_pairs) *near_cell_tri_pairs = mesh->m->h.near_cell_tri_pairs;
   return EB_OK;
 }
 

@@ -158,6 +158,32 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v)
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Columns of every 16 whose reciprocal square root runs on the FMA pipe
+// instead of MUFU (MUFU is the tensor-core kernel's only saturated pipe; the
+// FMA pipe has half its time left).
+#ifndef EB_TC_NEWTON
+#define EB_TC_NEWTON 0
+#endif
+constexpr int kNewtonPer16 = EB_TC_NEWTON;
+static_assert(kNewtonPer16 % 2 == 0 && kNewtonPer16 <= 16, "Newton columns come in pairs");
+
+// 1/sqrt(x) of two values on the FMA pipe: the magic-constant seed of the
+// "fast inverse square root" (constant 0x5f375a86 from C. Lomont, "Fast
+// Inverse Square Root", 2003; relative error < 3.5e-2) and three Newton
+// steps y <- y (3/2 - x/2 y^2), which square the error each time (below the
+// FP32 rounding after the third). 2 integer and 10 FP32 lane operations per
+// value.
+__device__ __forceinline__ float2 rsqrt2_newton(float2 x)
+{
+  float2 y = make_float2(__int_as_float(0x5f375a86 - (__float_as_int(x.x) >> 1)),
+                         __int_as_float(0x5f375a86 - (__float_as_int(x.y) >> 1)));
+  const float2 hx = __fmul2_rn(make_float2(-0.5f, -0.5f), x);
+  const float2 c15 = make_float2(1.5f, 1.5f);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) y = __fmul2_rn(y, __ffma2_rn(hx, __fmul2_rn(y, y), c15));
+  return y;
+}
+
 // byte offset of (row, 16-byte K group) in the UMMA K-major no-swizzle layout
 __host__ __device__ constexpr int umma_off(int row, int kg) { return (row >> 3) * 512 + kg * 128 + (row & 7) * 16; }
 
@@ -444,7 +470,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             for (int j = 0; j < kMax; j += 2) {
               if (j >= 8 * nb) break;
               const float2 cj = *reinterpret_cast<const float2*>(cc2 + h0 + j);
-              const float2 ri = make_float2(rsq(vd[j]), rsq(vd[j + 1]));
+              const float2 ri = (j % 16) >= 16 - kNewtonPer16 ? rsqrt2_newton(make_float2(vd[j], vd[j + 1]))
+                                                              : make_float2(rsq(vd[j]), rsq(vd[j + 1]));
               sl2 = __ffma2_rn(cj, ri, sl2);
               dl2 = __ffma2_rn(__fmul2_rn(ri, ri), __fmul2_rn(make_float2(ve[j], ve[j + 1]), ri), dl2);
             }

@@ -43,6 +43,11 @@ struct HostMesh {
   std::vector<int> dl_contrib_ptr, dl_contrib;  // slot -> entries, ascending
 
   long long far_quad_pairs = 0;  // regular quadrature-point pairs per apply
+  // (target item, source triangle) pairs in source cells well separated from
+  // the item's target tile, and in the others (where a far-field kernel
+  // masks vertex-sharing pairs and forms differences directly); set with the
+  // static tables
+  long long far_cell_tri_pairs = 0, near_cell_tri_pairs = 0;
 };
 
 // Validates and prepares; returns EB_OK or an error status with a message.
