@@ -1,4 +1,5 @@
 #include "batch.h"
+#include "farfield_tc.h"
 
 #include <algorithm>
 #include <numeric>
@@ -52,6 +53,10 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   Q_ = entries[0]->mesh->h.Q;
   K_ = entries[0]->mesh->h.K;
   const int n = (int)entries.size();
+  tc_ = fp32 && nsl_ == 1 && nd_ == 1;
+  for (BatchEntry* be : entries) tc_ = tc_ && tc_eligible(be->mesh, fp32, 1, 1);
+  std::vector<TcPrepArgs> targs;
+  std::vector<int> toff(1, 0);
   std::vector<FarMeshDesc> desc(n);
   std::vector<ApplyArgs> args(n);
   std::vector<int> poff(n + 1, 0), foff(n + 1, 0);
@@ -68,6 +73,17 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     if (nd_ && !be->uin.p) return set_error(EB_ERR_INVALID, "batch entry without DL columns");
     desc[e] = mesh_far_desc(m, fp32, nsl_, nd_, be->rec.p, be->partial.as<double>());
     desc[e].active = d_flags ? d_flags + e : nullptr;
+    if (tc_) {
+      EB_CHECK(ensure_tc_static(m));
+      EB_CHECK(be->tc_be.alloc(far_tc_operand_bytes(h.ncells)));
+      EB_CHECK(be->tc_charge.alloc(far_tc_charge_bytes(h.ncells)));
+      desc[e].tc_bd2 = m->tc_bd2.as<float4>();
+      desc[e].tc_be = be->tc_be.as<float4>();
+      desc[e].tc_charge = be->tc_charge.as<float>();
+      targs.push_back(TcPrepArgs{h.ne, h.ncells, be->rec.as<float4>(), m->splane32.as<float4>(),
+                                 be->tc_be.as<float4>(), be->tc_charge.as<float>(), desc[e].active});
+      toff.push_back(toff.back() + far_tc_prep_blocks(h.ncells));
+    }
     src_tile = std::min(src_tile, desc[e].src_tile);
     args[e] = mesh_apply_args(m, fp32, be->rec.p, be->partial.as<double>(), nsl_ ? be->tin.as<double>() : nullptr,
                               h.ne, nd_ ? be->uin.as<double>() : nullptr, nsl_ ? be->vout.as<double>() : nullptr,
@@ -106,6 +122,15 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   EB_CHECK(fin_off_.alloc(sizeof(int) * (n + 1)));
   EB_CHECK(copy_h2d(fin_off_.p, foff.data(), sizeof(int) * (n + 1)));
   EB_CHECK(counter_.alloc(sizeof(int)));
+  if (tc_) {
+    EB_CHECK(tc_args_.alloc(sizeof(TcPrepArgs) * n));
+    EB_CHECK(copy_h2d(tc_args_.p, targs.data(), sizeof(TcPrepArgs) * n));
+    EB_CHECK(tc_off_.alloc(sizeof(int) * (n + 1)));
+    EB_CHECK(copy_h2d(tc_off_.p, toff.data(), sizeof(int) * (n + 1)));
+    EB_CHECK(tc_err_.alloc(sizeof(int)));
+    EB_CHECK(memset_sync(tc_err_.p, 0, sizeof(int)));
+    tc_blocks_ = toff[n];
+  }
 
   smem_ = far_smem_bytes(src_tile, Q_, rec_slots(nsl_, nd_), fp32);
   int occ = far_occupancy(fp32, nsl_, nd_, K_, Q_, smem_);
@@ -116,7 +141,21 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   grid_ = std::min(nsm * occ, std::max(1, nitems_));
   occ_ = occ;
   nsm_ = nsm;
+  if (tc_) {  // one 256-thread CTA per SM holding all of its tensor memory
+    grid_ = std::min(nsm, std::max(1, nitems_));
+    occ_ = 1;
+  }
   return EB_OK;
+}
+
+int Batch::check_error()
+{
+  if (!tc_ || !tc_err_.p) return EB_OK;
+  int flag = 0;
+  EB_CHECK(copy_d2h(&flag, tc_err_.p, sizeof(int)));
+  if (!flag) return EB_OK;
+  EB_CHECK(memset_sync(tc_err_.p, 0, sizeof(int)));
+  return set_error(EB_ERR_TIMEOUT, "tensor-core far field: a bounded wait for the tensor cores ran out");
 }
 
 int Batch::run(cudaStream_t st, int reserve_sms)
@@ -126,9 +165,14 @@ int Batch::run(cudaStream_t st, int reserve_sms)
   const int free_sms = std::max(1, nsm_ - std::max(0, reserve_sms));
   const int grid = reserve_sms > 0 ? std::min(grid_, free_sms * occ_) : grid_;
   EB_CUDA(prep_launch_batch(fp32_, nsl_, nd_, args_.as<ApplyArgs>(), prep_off_.as<int>(), n, prep_blocks_, st));
+  if (tc_) EB_CUDA(far_tc_prep_dl_batch(tc_args_.as<TcPrepArgs>(), tc_off_.as<int>(), n, tc_blocks_, st));
   EB_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(int), st));
-  EB_CUDA(far_launch(fp32_, nsl_, nd_, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
-                     counter_.as<int>(), smem_, grid, st));
+  if (tc_)
+    EB_CUDA(far_tc_launch(desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(),
+                          tc_err_.as<int>(), grid, st));
+  else
+    EB_CUDA(far_launch(fp32_, nsl_, nd_, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
+                       counter_.as<int>(), smem_, grid, st));
   EB_CUDA(finalize_launch_batch(nsl_, nd_, args_.as<ApplyArgs>(), fin_off_.as<int>(), n, fin_blocks_, st));
   return EB_OK;
 }
@@ -252,7 +296,10 @@ int eb_batch_apply_sl_dl(eb_batch b, const double* const* d_t, const double* con
     EB_CUDA(cudaMemcpyAsync(d_v[i], e.vout.p, sizeof(double) * e.mesh->h.ne, cudaMemcpyDeviceToDevice, st));
     EB_CUDA(cudaMemcpyAsync(d_q[i], e.qout.p, sizeof(double) * e.mesh->h.ne, cudaMemcpyDeviceToDevice, st));
   }
-  if (!stream) EB_CUDA(cudaStreamSynchronize(st));
+  if (!stream) {
+    EB_CUDA(cudaStreamSynchronize(st));
+    EB_CHECK(b->batch.check_error());
+  }
   return EB_OK;
 }
 

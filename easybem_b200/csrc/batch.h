@@ -27,6 +27,7 @@ struct BatchEntry {
   DevBuf rec, partial;  // apply scratch
   DevBuf tin, vout;     // kBatchCols columns of nelems each (inputs / outputs)
   DevBuf uin, qout;     // DL density [nnodes] and DL output [nelems] (batches with a DL column)
+  DevBuf tc_be, tc_charge;  // tensor-core DL operand and charges (tensor-core SL+DL batches)
   int index = -1;       // position in the current batch
 };
 
@@ -50,6 +51,10 @@ class Batch {
   ~Batch() { reset_graph(); }
 
   int nentries() const { return (int)entries_.size(); }
+  bool tensor_cores() const { return tc_; }
+  // EB_ERR_TIMEOUT (flag cleared) if the last tensor-core launch gave up a
+  // bounded wait; the batch's stream must be synchronised.
+  int check_error();
   long long quad_pairs() const { return quad_pairs_; }
 
  private:
@@ -58,6 +63,9 @@ class Batch {
   int nsl_ = kBatchCols;
   int nd_ = 0;
   DevBuf desc_, items_, args_, prep_off_, fin_off_, counter_;
+  bool tc_ = false;  // far field on the tensor cores (fused FP32 SL+DL, 7-point rule, engine 1 on every mesh)
+  DevBuf tc_args_, tc_off_, tc_err_;
+  int tc_blocks_ = 0;
   int nitems_ = 0, grid_ = 0, occ_ = 1, nsm_ = 148, prep_blocks_ = 0, fin_blocks_ = 0, K_ = 0, Q_ = 0;
   size_t smem_ = 0;
   long long quad_pairs_ = 0;

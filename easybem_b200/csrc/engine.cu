@@ -647,17 +647,30 @@ bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd)
 
 // The tensor-core far field: static operands once per mesh, then per apply
 // the DL operand and charges from the records, the persistent kernel.
+int ensure_tc_static(Mesh* m)
+{
+  if (m->tc_static_ready) return EB_OK;
+  const HostMesh& h = m->h;
+  EB_CHECK(m->tc_bd2.alloc(far_tc_operand_bytes(h.ncells)));
+  int dev = 0;
+  EB_CUDA(cudaGetDevice(&dev));
+  cudaStream_t st = pool_stream(dev);
+  if (!st) return set_error(EB_ERR_CUDA, "cannot create the staging stream");
+  EB_CUDA(far_tc_prep_static(h.ne, h.ncells, m->pos32.as<float4>(), m->tc_bd2.as<float4>(), st));
+  EB_CUDA(cudaStreamSynchronize(st));
+  m->tc_static_ready = true;
+  return EB_OK;
+}
+
 static int tc_far_apply(Mesh* m, cudaStream_t st)
 {
   const HostMesh& h = m->h;
-  if (!m->tc_static_ready) {
-    EB_CHECK(m->tc_bd2.alloc(far_tc_operand_bytes(h.ncells)));
+  EB_CHECK(ensure_tc_static(m));
+  if (!m->tc_err.p) {  // the single-mesh apply's DL operand, charges and error flag
     EB_CHECK(m->tc_be.alloc(far_tc_operand_bytes(h.ncells)));
     EB_CHECK(m->tc_charge.alloc(far_tc_charge_bytes(h.ncells)));
     EB_CHECK(m->tc_err.alloc(sizeof(int)));
     EB_CHECK(memset_sync(m->tc_err.p, 0, sizeof(int)));
-    EB_CUDA(far_tc_prep_static(h.ne, h.ncells, m->pos32.as<float4>(), m->tc_bd2.as<float4>(), st));
-    m->tc_static_ready = true;
   }
   if (!m->tc_var.desc.p) {  // (re)built after a plan change: scratch pointers and split
     FarMeshDesc desc = mesh_far_desc(m, true, 1, 1, m->rec.p, m->partial.as<double>());

@@ -159,6 +159,8 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
 // True when mesh m applies the fused FP32 SL+DL far field with the
 // tensor-core kernel (engine 1, 7-point rule).
 bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd);
+// The tensor-core distance operand of m (built once, synchronously).
+int ensure_tc_static(Mesh* m);
 // EB_ERR_TIMEOUT (and the flag cleared) if the last tensor-core launch on m
 // gave up a bounded wait; EB_OK otherwise. The stream must be synchronised.
 int mesh_check_far_error(Mesh* m);

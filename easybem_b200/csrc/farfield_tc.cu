@@ -230,10 +230,10 @@ __global__ void tc_prep_static_kernel(int ne, int ncells, const float4* __restri
 }
 
 // records of the fused SL+DL FP32 variant: slot1 = (s, c, 0, 0)
-__global__ void tc_prep_dl_kernel(int ne, int ncells, const float4* __restrict__ rec, const float4* __restrict__ splane32,
-                                  float4* __restrict__ be, float* __restrict__ charges)
+__device__ __forceinline__ void tc_prep_dl_point(int idx, int ne, int ncells, const float4* __restrict__ rec,
+                                                 const float4* __restrict__ splane32, float4* __restrict__ be,
+                                                 float* __restrict__ charges)
 {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= ncells * tc::kCellPts) return;
   const int c = idx / tc::kCellPts, p = idx % tc::kCellPts;
   float row[16];
@@ -263,6 +263,26 @@ __global__ void tc_prep_dl_kernel(int ne, int ncells, const float4* __restrict__
     *reinterpret_cast<float4*>(base + tc::umma_off(p, kg)) =
         make_float4(row[4 * kg], row[4 * kg + 1], row[4 * kg + 2], row[4 * kg + 3]);
   charges[idx] = charge;
+}
+
+__global__ void tc_prep_dl_kernel(int ne, int ncells, const float4* __restrict__ rec, const float4* __restrict__ splane32,
+                                  float4* __restrict__ be, float* __restrict__ charges)
+{
+  tc_prep_dl_point(blockIdx.x * blockDim.x + threadIdx.x, ne, ncells, rec, splane32, be, charges);
+}
+
+__global__ void tc_prep_dl_batch_kernel(const TcPrepArgs* __restrict__ args, const int* __restrict__ off, int n)
+{
+  int lo = 0, hi = n;  // off[lo] <= blockIdx.x < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= (int)blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  const TcPrepArgs A = args[lo];
+  if (A.active && *A.active == 0) return;
+  tc_prep_dl_point((blockIdx.x - off[lo]) * blockDim.x + threadIdx.x, A.ne, A.ncells, A.rec, A.splane32, A.be,
+                   A.charges);
 }
 
 __global__ void __launch_bounds__(tc::kThreads, 1)
@@ -536,6 +556,12 @@ cudaError_t far_tc_prep_dl(int ne, int ncells, const float4* rec, const float4* 
 {
   const int n = ncells * tc::kCellPts;
   tc_prep_dl_kernel<<<(n + 255) / 256, 256, 0, st>>>(ne, ncells, rec, splane32, be, charges);
+  return cudaGetLastError();
+}
+
+cudaError_t far_tc_prep_dl_batch(const TcPrepArgs* d_args, const int* d_off, int n, int nblocks, cudaStream_t st)
+{
+  if (nblocks > 0) tc_prep_dl_batch_kernel<<<nblocks, 256, 0, st>>>(d_args, d_off, n);
   return cudaGetLastError();
 }
 

@@ -22,6 +22,20 @@ cudaError_t far_tc_prep_static(int ne, int ncells, const float4* pos32, float4* 
 // DL-GEMM source operand and the SL charges.
 cudaError_t far_tc_prep_dl(int ne, int ncells, const float4* rec, const float4* splane32, float4* be, float* charges,
                            cudaStream_t st);
+// Per-entry arguments of the batched DL-operand preparation.
+struct TcPrepArgs {
+  int ne, ncells;
+  const float4* rec;       // records of the fused FP32 variant
+  const float4* splane32;  // n_j and the cell-relative plane offset
+  float4* be;              // DL-GEMM source operand out
+  float* charges;          // SL charges out
+  const int* active;       // optional: skip while *active == 0
+};
+// Blocks [off[e], off[e+1]) of 256 threads prepare entry e.
+cudaError_t far_tc_prep_dl_batch(const TcPrepArgs* d_args, const int* d_off, int n, int nblocks, cudaStream_t st);
+// Thread blocks of 256 points far_tc_prep_dl_batch needs for a mesh.
+inline int far_tc_prep_blocks(int ncells) { return (ncells * kCell * kTcRule + 255) / 256; }
+
 // The persistent kernel (grid = SM count); *d_error becomes 1 if a bounded
 // wait ran out.
 cudaError_t far_tc_launch(const FarMeshDesc* d_meshes, const WorkItem* d_items, int nitems, int* d_counter,
