@@ -155,3 +155,76 @@ def test_oracle_matches_golden_at_reference_driver_orders(oracle):
         assert rel_l2(v, vg[sel]) < 1e-13, (name, o)
         assert rel_l2(q, qg[sel]) < 1e-13, (name, o)
     oracle.set_order(4)
+
+
+def _p1_by_vertex(oracle, nodes, elems, i, j):
+    """The oracle's 9 P1 integrals of pair (i, j) keyed by (test vertex, trial vertex)."""
+    ok, I, ti, tj = oracle.p1_pair(nodes, elems, i, j)
+    assert ok
+    return {(int(ti[k]), int(tj[l])): I[k, l] for k in range(3) for l in range(3)}
+
+
+def test_p1_disjoint_pairs_match_independent_quadrature(oracle):
+    # Every basis-pair integral of well-separated triangles, against a plain
+    # tensor-product evaluation of sum_a sum_b w_a w_b J_i J_j phi_k(x_a)
+    # phi_l(y_b) / (4 pi |x_a - y_b|) with the same triangle rule (the
+    # reference's P1 formulas are restated from its GPU kernels; this checks
+    # them entry by entry, not only through their sum).
+    nodes, elems = meshes.perturbed_icosphere(2, seed=3)
+    f = elems - 1
+    for order in (4, 18):
+        oracle.set_order(order)
+        r = O.reference_rules(order)
+        xi, eta, w = r["tx"], r["ty"], r["tw"]
+        phi = np.stack([1.0 - xi - eta, xi, eta])  # [3, Q]
+        rng = np.random.default_rng(order)
+        checked = 0
+        while checked < 40:
+            i, j = rng.integers(0, elems.shape[0], size=2)
+            if set(f[i]) & set(f[j]):
+                continue
+            Pi, Pj = nodes[f[i]], nodes[f[j]]
+            x = Pi[0] + np.outer(xi, Pi[1] - Pi[0]) + np.outer(eta, Pi[2] - Pi[0])
+            y = Pj[0] + np.outer(xi, Pj[1] - Pj[0]) + np.outer(eta, Pj[2] - Pj[0])
+            Ji = np.linalg.norm(np.cross(Pi[1] - Pi[0], Pi[2] - Pi[0]))
+            Jj = np.linalg.norm(np.cross(Pj[1] - Pj[0], Pj[2] - Pj[0]))
+            G = 1.0 / (4 * np.pi * np.linalg.norm(x[:, None, :] - y[None, :, :], axis=2))
+            ref = Ji * Jj * np.einsum("ka,a,ab,b,lb->kl", phi, w, G, w, phi)
+            got = _p1_by_vertex(oracle, nodes, elems, i, j)
+            for k in range(3):
+                for l in range(3):
+                    assert abs(got[(f[i][k], f[j][l])] - ref[k, l]) <= 1e-13 * abs(ref).max()
+            checked += 1
+    oracle.set_order(4)
+
+
+def test_p1_singular_pairs_converge_and_swap_symmetrically(oracle):
+    # Coincident, edge- and vertex-adjacent pairs: every basis-pair integral
+    # converges as the quadrature index grows, and the converged values obey
+    # the symmetry of the exact Galerkin integrals, I_ij[k][l] = I_ji[l][k]
+    # (the swapped pair is computed with another parametrisation and local
+    # vertex rotation, so this checks each entry independently).
+    nodes, elems = meshes.perturbed_icosphere(2, seed=3)
+    f = elems - 1
+    cases = {}  # shared vertices -> a triangle sharing that many with triangle 0
+    for j in range(1, elems.shape[0]):
+        cases.setdefault(len(set(f[0]) & set(f[j])), j)
+    assert {1, 2} <= set(cases)
+    pairs = [(0, 0), (0, cases[1]), (0, cases[2])]
+    hi = {}
+    oracle.set_order(18)
+    for i, j in pairs:
+        hi[(i, j)] = _p1_by_vertex(oracle, nodes, elems, i, j)
+        hi[(j, i)] = _p1_by_vertex(oracle, nodes, elems, j, i)
+    for i, j in pairs:
+        scale = max(abs(v) for v in hi[(i, j)].values())
+        for (a, b), v in hi[(i, j)].items():
+            assert abs(v - hi[(j, i)][(b, a)]) <= 1e-9 * scale, (i, j, a, b)
+        errs = []
+        for order in (6, 10, 14, 16):
+            oracle.set_order(order)
+            lo = _p1_by_vertex(oracle, nodes, elems, i, j)
+            errs.append(max(abs(lo[k] - hi[(i, j)][k]) for k in lo) / scale)
+        print(f"P1 pair ({i},{j}): max relative change to index 18 at indices 6/10/14/16: {errs}")
+        assert errs[-1] <= 1e-10 and errs[0] > errs[-1], (i, j, errs)
+    oracle.set_order(4)
