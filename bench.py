@@ -72,6 +72,9 @@ def parse_args(argv=None):
     p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
     p.add_argument("--serve-sample", type=int, default=300,
                    help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
+    p.add_argument("--far-engine", default="tensor", choices=["tensor", "cuda"],
+                   help="matvec: far field of the mixed apply on the tensor cores (tcgen05 distance GEMMs) or on "
+                        "the FP32 pipes only; the other engine is timed beside it")
     p.add_argument("--no-extras", action="store_true",
                    help="matvec: skip the batch (256 ellipsoids), large (L7) and small (L3 solve) records "
                         "that a one-GPU run adds to its line")
@@ -285,13 +288,17 @@ def batch_record(local, solves=True):
         return a.elapsed_time(b) / k
 
     out = {}
-    for prec in ("mixed", "fp64"):
+    for key, prec, engine in (("mixed", "mixed", "tensor"), ("mixed_cuda", "mixed", "cuda"), ("fp64", "fp64", "cuda")):
+        for m in ms:
+            m.set_far_engine(engine)
         bt = eb.Batch(ms, precision=prec, sl_dl=True)
         ms_apply = time_batch(bt, lambda b: b.apply_sl_dl_device(ptrs(d_t), ptrs(d_u), ptrs(d_v), ptrs(d_q),
                                                                   st.cuda_stream), 3 if prec == "mixed" else 2)
-        out[prec] = {"ms_per_apply": ms_apply, "Gpairs_per_s": bt.quad_pairs / (ms_apply * 1e-3) / 1e9}
-        out[prec + "_vq"] = (torch.cat(d_v).cpu().numpy(), torch.cat(d_q).cpu().numpy())
+        out[key] = {"engine": engine, "ms_per_apply": ms_apply, "Gpairs_per_s": bt.quad_pairs / (ms_apply * 1e-3) / 1e9}
+        out[key + "_vq"] = (torch.cat(d_v).cpu().numpy(), torch.cat(d_q).cpu().numpy())
         bt.close()
+    for m in ms:
+        m.set_far_engine("tensor")
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     mixed_vs_fp64 = {"sl": rel(out["mixed_vq"][0], out["fp64_vq"][0]), "dl": rel(out["mixed_vq"][1], out["fp64_vq"][1])}
     # sampled rows of 8 meshes against the CPU oracle
@@ -320,8 +327,9 @@ def batch_record(local, solves=True):
     rec = {"workload": "256 ellipsoids (icosphere L2-L5, 320-20,480 triangles), SL+DL batched apply "
                        "(one density pair per mesh), 4-RHS SL batched apply, GMRES(50)-IR to 1e-8",
            "quad_pairs_per_apply": int(pairs), "mesh_setup_s": t_create,
-           "sl_dl_mixed": out["mixed"], "sl_dl_fp64": out["fp64"],
+           "sl_dl_mixed": out["mixed"], "sl_dl_mixed_cuda_cores": out["mixed_cuda"], "sl_dl_fp64": out["fp64"],
            "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
+           "mixed_cuda_cores_over_fp64": out["mixed_cuda"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "rel_err_vs_oracle": err,
            "sl_4rhs_mixed": {"ms_per_apply": ms4, "Gpairs_per_s": pairs / (ms4 * 1e-3) / 1e9,
                              "rhs_evals_per_s_G": 4 * pairs / (ms4 * 1e-3) / 1e9}}
@@ -361,9 +369,11 @@ def large_record(local, solve=False):
     t_create = time.perf_counter() - t0
     m.set_profiling(True)
     res = {}
-    for prec in ("mixed", "fp64"):
-        m.apply_sl_dl(t, u, precision=prec)
-        v, q = m.apply_sl_dl(t, u, precision=prec)
+    for prec, engine in (("mixed_cuda", "cuda"), ("fp64", "cuda"), ("mixed", "tensor")):
+        m.set_far_engine(engine)
+        p = "fp64" if prec == "fp64" else "mixed"
+        m.apply_sl_dl(t, u, precision=p)
+        v, q = m.apply_sl_dl(t, u, precision=p)
         far, fin = m.last_kernel_ms()
         res[prec] = (v, q, far, fin)
     rng = np.random.default_rng(5)
@@ -373,11 +383,22 @@ def large_record(local, solve=False):
     pairs = m.far_quad_pairs
     peak_tflops, peak_rsqrt = _measure_peak()
     rate = pairs / (res["mixed"][2] * 1e-3)
-    bound = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
+    mufu_pp, fma_pp, _ = _engine_costs("tensor")
+    bound = min(peak_tflops * 1e12 / (2 * fma_pp), peak_rsqrt * 1e12 / mufu_pp)
+    rate_c = pairs / (res["mixed_cuda"][2] * 1e-3)
+    bound_c = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
+    cf, cn = m.cell_pairs()
     rec = {"workload": "radius-perturbed icosphere L7 (327,680 triangles, 163,842 vertices)",
            "quad_pairs_per_step": pairs, "near_pairs": m.near_pairs, "mesh_setup_s": t_create,
-           "mixed": {"far_ms": res["mixed"][2], "finalize_ms": res["mixed"][3], "Gpairs_per_s": rate / 1e9,
-                     "fma_pipe_frac": rate * FLOPS_PER_PAIR / (peak_tflops * 1e12), "frac_of_pair_bound": rate / bound},
+           "near_cell_share": cn / (cf + cn),
+           "mixed": {"engine": "tensor", "far_ms": res["mixed"][2], "finalize_ms": res["mixed"][3],
+                     "Gpairs_per_s": rate / 1e9, "mufu_frac": rate * mufu_pp / (peak_rsqrt * 1e12),
+                     "frac_of_pair_bound": rate / bound},
+           "mixed_cuda_cores": {"far_ms": res["mixed_cuda"][2], "Gpairs_per_s": rate_c / 1e9,
+                                "fma_pipe_frac": rate_c * FLOPS_PER_PAIR / (peak_tflops * 1e12),
+                                "frac_of_pair_bound": rate_c / bound_c,
+                                "rel_err_sl": rel(res["mixed_cuda"][0][rows], vo),
+                                "rel_err_dl": rel(res["mixed_cuda"][1][rows], qo)},
            "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
                     "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
            "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed"][0][rows], vo), "mixed_dl": rel(res["mixed"][1][rows], qo),
@@ -511,7 +532,8 @@ def main():
         ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
         return ms, far_ms
 
-    # launch plan: tuned on this mesh before any timing (untimed setup)
+    # launch plan: tuned on this mesh for the chosen engine before any timing (untimed setup)
+    mesh.set_far_engine(args.far_engine)
     plan = None if args.no_autotune else mesh.autotune(precision="mixed", operators="sl+dl", reps=2)
     plan_info = dict(mesh.plan(), tuned=plan is not None)
     if plan is not None:
@@ -527,6 +549,13 @@ def main():
     ms_fp64, far_fp64 = timed("fp64", k64, 1)
     v_64 = d_v.cpu().numpy()
     q_64 = d_q.cpu().numpy()
+    # the other far-field engine of the mixed apply, same plan
+    other = "cuda" if args.far_engine == "tensor" else "tensor"
+    mesh.set_far_engine(other)
+    ms_other, far_other = timed("mixed", max(2, args.steps // 3), 1)
+    v_other = d_v.cpu().numpy()
+    q_other = d_q.cpu().numpy()
+    mesh.set_far_engine(args.far_engine)
 
     step_ms = max_over_ranks(sum(ms_mixed) / len(ms_mixed), dist, dev)
     step_ms64 = max_over_ranks(sum(ms_fp64) / len(ms_fp64), dist, dev)
@@ -574,12 +603,16 @@ def main():
     # roofline of the dominant kernel (far field), event-timed on its stream
     far_avg = sum(f for f, _ in far_mixed) / len(far_mixed)
     fin_avg = sum(g for _, g in far_mixed) / len(far_mixed)
+    far_other_avg = sum(f for f, _ in far_other) / len(far_other)
     peak_tflops, peak_rsqrt = _measure_peak()
+    costs = {e: _engine_costs(e) for e in ("tensor", "cuda")}
+    mufu_pp, fma_pp, tc_pp = costs[args.far_engine]
     pair_rate = pairs / (far_avg * 1e-3)
-    achieved = pair_rate * FLOPS_PER_PAIR / 1e12
-    mufu = pair_rate * RSQRT_PER_PAIR / 1e12
-    # the pair rate both pipes allow together, and the fraction of it reached
-    pair_bound = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
+    # pipe rates at this pair rate, and the pair rate the measured pipe peaks allow
+    fma_tflops = pair_rate * 2 * fma_pp / 1e12
+    mufu = pair_rate * mufu_pp / 1e12
+    pair_bound = min(peak_tflops * 1e12 / (2 * fma_pp), peak_rsqrt * 1e12 / mufu_pp)
+    cell_far, cell_near = mesh.cell_pairs()
     nb = ctypes.c_longlong()
     _lib.check(L.eb_mesh_finalize_bytes(mesh.handle, ctypes.byref(nb)))
     near_bytes = nb.value  # near-field CSR + gathered densities + far partial sums + outputs
@@ -610,20 +643,33 @@ def main():
         "fp64": {"value": value64, "unit": "Gpairs/s", "ms_per_step": step_ms64, "steps": len(ms_fp64),
                  "far_ms": sum(f for f, _ in far_fp64) / len(far_fp64)},
         "mixed_over_fp64": value / value64,
+        "far_engine": args.far_engine,
+        "other_engine": {"engine": other, "ms_per_step": sum(ms_other) / len(ms_other), "far_ms": far_other_avg,
+                         "Gpairs_per_s": pairs / (far_other_avg * 1e-3) / 1e9,
+                         "rel_err_vs_oracle": {"sl": rel(v_other[rows], vo), "dl": rel(q_other[rows], qo)},
+                         "note": "the mixed apply with the other far-field engine, same plan and inputs"},
+        "near_cell_share": cell_near / (cell_far + cell_near),
         "rel_err_vs_oracle": err,
         "e2e": {"value": e2e_value, "unit": "Gpairs/s", "h2d_bytes_per_step": 8 * (ne + nv),
                 "d2h_bytes_per_step": 16 * ne, "ms_per_step": 1e3 * e2e_s},
-        "gpu_launches": 3 * args.steps,
-        "roofline": {"bound": "fp32 (FMA pipe and MUFU)", "achieved": achieved, "peak": peak_tflops,
-                     "unit": "TFLOP/s", "frac": achieved / peak_tflops if peak_tflops else None,
-                     "traffic": FAR_TRAFFIC_L6 if args.level == LEVEL else None, "traffic_unit": "bytes per launch",
-                     "kernel": "far_kernel<float,7,7,1,true>", "far_ms": far_avg,
-                     "flops_per_pair": FLOPS_PER_PAIR,
+        "gpu_launches": (4 if args.far_engine == "tensor" else 3) * args.steps,
+        "roofline": {"bound": ("MUFU reciprocal square root (tensor cores carry the distance GEMMs)"
+                               if args.far_engine == "tensor" else "FMA pipe and MUFU together"),
+                     "achieved": pair_rate / 1e9, "peak": pair_bound / 1e9, "unit": "Gpairs/s",
+                     "frac": pair_rate / pair_bound,
+                     "traffic": FAR_TRAFFIC_L6 if (args.level == LEVEL and args.far_engine == "cuda") else None,
+                     "traffic_unit": "bytes per launch",
+                     "kernel": "far_tc_kernel" if args.far_engine == "tensor" else "far_kernel<float,7,7,1,true>",
+                     "far_ms": far_avg,
+                     "per_pair": {"mufu_rsqrt": mufu_pp, "fma_pipe_ops": fma_pp, "tensor_flops": tc_pp},
+                     "fma": {"achieved": fma_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
+                             "frac": fma_tflops / peak_tflops if peak_tflops else None},
                      "mufu": {"achieved": mufu, "peak": peak_rsqrt, "unit": "Trsqrt/s",
                               "frac": mufu / peak_rsqrt if peak_rsqrt else None},
-                     "pair_bound_Gpairs_s": pair_bound / 1e9, "frac_of_pair_bound": pair_rate / pair_bound,
-                     "peak_source": "FFMA-chain and MUFU rsqrt-chain calibration kernels measured in this run "
-                                    "(8 FMA-pipe ops = 16 flops and 1 rsqrt per quadrature pair)"},
+                     "tensor_tflops_tf32": pair_rate * tc_pp / 1e12,
+                     "peak_source": "FFMA-chain and MUFU rsqrt-chain calibration kernels measured in this run; "
+                                    "peak = the pair rate those two measured pipe peaks allow at the kernel's "
+                                    "per-pair pipe work (eb_far_engine_costs)"},
         "near_field": {"kernel": "finalize_kernel<1,1> (near-field SpMV + partial-sum fold)",
                        "finalize_ms": fin_avg, "algorithmic_bytes": near_bytes,
                        "spmv_bytes": nb_spmv.value, "fold_bytes": nb_fold.value,
@@ -667,6 +713,15 @@ def _hbm_peak():
             return json.load(fh).get("hbm_gbs")
     except (OSError, ValueError):
         return None
+
+
+def _engine_costs(engine):
+    import ctypes
+    from easybem_b200 import _lib
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.lib().eb_far_engine_costs({"cuda": 0, "tensor": 1}[engine], ctypes.byref(a), ctypes.byref(b),
+                                              ctypes.byref(c)))
+    return a.value, b.value, c.value
 
 
 def _measure_peak():

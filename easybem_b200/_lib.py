@@ -38,6 +38,8 @@ _SIGNATURES = {
     "eb_mesh_info": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "eb_mesh_finalize_bytes": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_far_engine_costs": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double)]),
     "eb_mesh_cell_pairs": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "eb_mesh_set_far_engine": (ctypes.c_int, [_dp, ctypes.c_int]),
     "eb_mesh_get_far_engine": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),

@@ -1040,6 +1040,20 @@ int eb_mesh_get_far_engine(eb_mesh mesh, int precision, int* engine)
   return EB_OK;
 }
 
+int eb_far_engine_costs(int engine, double* mufu_per_pair, double* fma_ops_per_pair, double* tensor_flops_per_pair)
+{
+  if (engine == EB_FAR_TENSOR_CORES) {
+    eb::far_tc_costs(mufu_per_pair, fma_ops_per_pair, tensor_flops_per_pair);
+  } else if (engine == EB_FAR_CUDA_CORES) {
+    if (mufu_per_pair) *mufu_per_pair = 1.0;
+    if (fma_ops_per_pair) *fma_ops_per_pair = 8.0;  // |x-y|^2 1 add + 3 FMA, SL 1 FMA, DL 2 mul + 1 FMA
+    if (tensor_flops_per_pair) *tensor_flops_per_pair = 0.0;
+  } else {
+    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES or EB_FAR_TENSOR_CORES");
+  }
+  return EB_OK;
+}
+
 int eb_set_profiling(eb_mesh mesh, int on)
 {
   if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");

@@ -544,6 +544,15 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
+void far_tc_costs(double* mufu_per_pair, double* fma_ops_per_pair, double* tensor_flops_per_pair)
+{
+  // per warpgroup round: kHalf columns, of which 3 x kNewtonPer16 take the FMA-pipe root
+  const double f = 3.0 * tc::kNewtonPer16 / tc::kHalf;
+  if (mufu_per_pair) *mufu_per_pair = 1.0 - f;
+  if (fma_ops_per_pair) *fma_ops_per_pair = 4.0 + 10.0 * f;  // SL 1, DL 3; Newton root 10
+  if (tensor_flops_per_pair) *tensor_flops_per_pair = 2.0 * 2.0 * 16.0;  // two GEMMs, K = 16, FMA = 2 flops
+}
+
 cudaError_t far_tc_prep_static(int ne, int ncells, const float4* pos32, float4* bd2, cudaStream_t st)
 {
   const int n = ncells * tc::kCellPts;

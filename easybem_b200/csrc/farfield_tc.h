@@ -16,6 +16,10 @@ constexpr int kTcRule = 7;     // triangle-rule points the kernel is built for (
 inline size_t far_tc_operand_bytes(int ncells) { return (size_t)ncells * kCell * kTcRule * 64; }
 inline size_t far_tc_charge_bytes(int ncells) { return (size_t)ncells * kCell * kTcRule * 4; }
 
+// Pipe work per far quadrature pair of the kernel as built: MUFU reciprocal
+// square roots, FMA-pipe lane operations, tensor-core flops.
+void far_tc_costs(double* mufu_per_pair, double* fma_ops_per_pair, double* tensor_flops_per_pair);
+
 // Once per mesh: the distance-GEMM source operand from the FP32 positions.
 cudaError_t far_tc_prep_static(int ne, int ncells, const float4* pos32, float4* bd2, cudaStream_t st);
 // Per apply, after the record preparation of the fused FP32 variant: the

@@ -338,6 +338,11 @@ int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit
 #define EB_FAR_TENSOR_CORES 1
 int eb_mesh_set_far_engine(eb_mesh mesh, int engine);
 int eb_mesh_get_far_engine(eb_mesh mesh, int precision, int* engine);
+/* Pipe work per well-separated quadrature pair of the fused mixed SL+DL far
+ * field on an engine, as this library was built: MUFU reciprocal square
+ * roots, FMA-pipe lane operations (an FMA counts once) and tensor-core
+ * flops (the numerators of the kernels' rooflines). */
+int eb_far_engine_costs(int engine, double* mufu_per_pair, double* fma_ops_per_pair, double* tensor_flops_per_pair);
 
 /* Times candidate plans (items_per_sm in {4,8,...,512} x source tile in
  * {default, 32, 16}) on this mesh with CUDA events, median of `reps` applies
