@@ -64,17 +64,25 @@ constexpr unsigned kWaitLimit = 1u << 20;      // try_wait calls before a wait g
 static_assert(kCellPts % kChunk == 0 && kChunk % 16 == 0, "chunk shape");
 static_assert(kTT == 128, "one tensor-memory lane per target triangle");
 
-// dynamic shared memory layout (bytes)
+// Source operands of the next well-separated cell of a work item are copied
+// into a second set of buffers (cp.async) while the current cell's rounds run.
+#ifndef EB_TC_PREFETCH
+#define EB_TC_PREFETCH 0
+#endif
+constexpr int kSets = EB_TC_PREFETCH ? 2 : 1;
+
+// dynamic shared memory layout (bytes); an operand set is (d2 operand, e
+// operand, charges) of one cell
 constexpr int kOffA = 0;                                   // 7 target operands
-constexpr int kOffB = kOffA + kQ * kABytes;                // d2 source operand of the cell
-constexpr int kOffE = kOffB + kCellBBytes;                 // e source operand of the cell
-constexpr int kOffC = kOffE + kCellBBytes;                 // SL charges of the cell
-constexpr int kOffRec = kOffC + kCellPts * 4;              // CUDA-core records of a near cell
+constexpr int kSetBytes = 2 * kCellBBytes + kCellPts * 4;  // 29,568
+constexpr int kOffSets = kOffA + kQ * kABytes;
+constexpr int kOffRec = kOffSets + kSets * kSetBytes;      // CUDA-core records of a near cell
 constexpr int kOffEnd = kOffRec + kCellPts * 2 * 16;
 // more than half of the SM's shared memory: one CTA per SM (it holds all
 // 512 tensor-memory columns)
-constexpr int kSmemBytes = 120 * 1024;
+constexpr int kSmemBytes = kSets == 1 ? 120 * 1024 : 124 * 1024;
 static_assert(kOffEnd <= kSmemBytes, "shared memory layout");
+static_assert(kSetBytes % 16 == 0, "16-byte aligned operand sets");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -157,6 +165,40 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v)
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copies cell `cell`'s d2 and e operands and charges into an operand set:
+// synchronously (ASYNC false) or with cp.async (committed as one group).
+template <bool ASYNC>
+__device__ __forceinline__ void load_cell_operands(unsigned char* set, const FarMeshDesc& md, int cell, int tid)
+{
+  const float4* gB = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(md.tc_bd2) + (size_t)cell * kCellBBytes);
+  const float4* gE = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(md.tc_be) + (size_t)cell * kCellBBytes);
+  const float4* gC = reinterpret_cast<const float4*>(md.tc_charge + (size_t)cell * kCellPts);
+  float4* sB = reinterpret_cast<float4*>(set);
+  float4* sE = reinterpret_cast<float4*>(set + kCellBBytes);
+  float4* sC = reinterpret_cast<float4*>(set + 2 * kCellBBytes);
+  for (int k = tid; k < kCellBBytes / 16; k += kThreads) {
+    if constexpr (ASYNC) {
+      cp_async16(sB + k, gB + k);
+      cp_async16(sE + k, gE + k);
+    } else {
+      sB[k] = gB[k];
+      sE[k] = gE[k];
+    }
+  }
+  for (int k = tid; k < kCellPts / 4; k += kThreads) {
+    if constexpr (ASYNC) cp_async16(sC + k, gC + k);
+    else sC[k] = gC[k];
+  }
+  if constexpr (ASYNC) cp_async_commit();
+}
 
 // Columns of every 16 whose reciprocal square root runs on the FMA pipe
 // instead of MUFU (MUFU is the tensor-core kernel's only saturated pipe; the
@@ -305,10 +347,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
   const int row = tid & 127;        // target triangle of the tile = tensor-memory lane
   const int warp = tid >> 5;
   unsigned char* sA = smem + kOffA;
-  unsigned char* sB = smem + kOffB;
-  unsigned char* sE = smem + kOffE;
-  float* sC = reinterpret_cast<float*>(smem + kOffC);
   float* sRec = reinterpret_cast<float*>(smem + kOffRec);
+  int set_cur = 0;  // operand set of the current far cell (uniform)
   const uint32_t mbar0 = smem_u32(&s_mbar[0]);
 
   if (warp == 0) {
@@ -355,13 +395,18 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     for (int a = 0; a < kQ; ++a) pw[a] = md.tgt32[(size_t)tsel * kQ + a].w;
     float acc_hi[2] = {0.f, 0.f}, acc_lo[2] = {0.f, 0.f};  // SL, DL
     const float4* rec = reinterpret_cast<const float4*>(md.rec);
+    auto is_far = [&](int c) {  // tile-level separation test: uniform across the CTA
+      const dq cc = md.ccent[c];
+      const double ddx = cc.x - tile.x, ddy = cc.y - tile.y, ddz = cc.z - tile.z;
+      const double rr = kFarRatio * (cc.w + tile.w);
+      return ddx * ddx + ddy * ddy + ddz * ddz > rr * rr;
+    };
+    int prefetched = -1;  // cell whose operands are in flight into set set_cur ^ 1
 
     for (int cell = w.cell0; cell < w.cell1; ++cell) {
       const int s0 = cell * kCell, s1 = min(md.ne, s0 + kCell);
       const dq cc = md.ccent[cell];
-      const double ddx = cc.x - tile.x, ddy = cc.y - tile.y, ddz = cc.z - tile.z;
-      const double rr = kFarRatio * (cc.w + tile.w);
-      const bool far = ddx * ddx + ddy * ddy + ddz * ddz > rr * rr;  // uniform across the CTA
+      const bool far = is_far(cell);
       const float o[3] = {(float)(cc.x - cen[0]), (float)(cc.y - cen[1]), (float)(cc.z - cen[2])};
       float xs[kQ], ys[kQ], zs[kQ], q2[kQ];
 #pragma unroll
@@ -421,22 +466,29 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             *reinterpret_cast<float4*>(dstA + umma_off(row, kg)) =
                 make_float4(v[4 * kg], v[4 * kg + 1], v[4 * kg + 2], v[4 * kg + 3]);
         }
-        // source operands and charges of the cell
-        {
-          const float4* gB = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(md.tc_bd2) +
-                                                             (size_t)cell * kCellBBytes);
-          const float4* gE = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(md.tc_be) +
-                                                             (size_t)cell * kCellBBytes);
-          for (int k = tid; k < kCellBBytes / 16; k += kThreads) {
-            reinterpret_cast<float4*>(sB)[k] = gB[k];
-            reinterpret_cast<float4*>(sE)[k] = gE[k];
-          }
-          for (int k = tid; k < kCellPts; k += kThreads) sC[k] = md.tc_charge[(size_t)cell * kCellPts + k];
+        // source operands and charges of the cell: already in flight into
+        // the other set, or copied now
+        if (kSets == 2 && prefetched == cell) {
+          set_cur ^= 1;
+          cp_async_wait_all();
+        } else {
+          load_cell_operands<false>(smem + kOffSets + set_cur * kSetBytes, md, cell, tid);
         }
+        prefetched = -1;
+        unsigned char* set = smem + kOffSets + set_cur * kSetBytes;
+        unsigned char* sB = set;
+        unsigned char* sE = set + kCellBBytes;
+        const float* sC = reinterpret_cast<const float*>(set + 2 * kCellBBytes);
         fence_async_smem();
         fence_before_sync();
         __syncthreads();
         fence_after_sync();
+        // the next cell's operands into the other set while these rounds run
+        // (that set's last reader, the previous far cell's MMAs, has completed)
+        if (kSets == 2 && cell + 1 < w.cell1 && is_far(cell + 1)) {
+          load_cell_operands<true>(smem + kOffSets + (set_cur ^ 1) * kSetBytes, md, cell + 1, tid);
+          prefetched = cell + 1;
+        }
         const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB), eBase = smem_u32(sE);
         auto issue = [&](int r) {
           const int a = r % kQ, ch = r / kQ;  // thread 0 only: runtime indices are fine here
@@ -507,6 +559,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         if (!ok) {
           if (tid == 0) atomicExch(error_flag, 1);
           s_stop = 1;
+          cp_async_wait_all();
           // wait (bounded) for the MMAs already issued before the memory is released
           for (int b = 0; b < 2; ++b) mbar_wait(mbar0 + 8 * b, (phase_bits >> b) & 1u);
           break;
