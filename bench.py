@@ -72,7 +72,7 @@ def parse_args(argv=None):
     p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
     p.add_argument("--serve-sample", type=int, default=300,
                    help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
-    p.add_argument("--far-engine", default="tensor", choices=["tensor", "cuda"],
+    p.add_argument("--far-engine", default="cuda", choices=["tensor", "cuda"],
                    help="matvec: far field of the mixed apply on the tensor cores (tcgen05 distance GEMMs) or on "
                         "the FP32 pipes only; the other engine is timed beside it")
     p.add_argument("--no-extras", action="store_true",

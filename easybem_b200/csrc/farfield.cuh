@@ -71,7 +71,10 @@ __host__ __device__ constexpr int charge_comp(int r, int nd) { return (r + nd) %
 // bounding-sphere centres exceeds kFarRatio times the sum of the radii (which
 // bound every vertex): no shared vertex is possible and |x|^2 + |y|^2 - 2 x.y
 // loses at most a few ulps to cancellation there.
-constexpr double kFarRatio = 2.5;
+#ifndef EB_FAR_RATIO
+#define EB_FAR_RATIO 2.5
+#endif
+constexpr double kFarRatio = EB_FAR_RATIO;
 
 // Per-mesh view used by the far-field kernels (device pointers).
 struct FarMeshDesc {
