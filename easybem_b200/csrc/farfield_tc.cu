@@ -32,8 +32,8 @@
 // Launch: one persistent CTA of 256 threads per SM (two warpgroups split
 // every 112-column chunk into halves of 56 columns), 512 tensor-memory
 // columns: two buffers x (d2, e) x 112. Round r = (chunk, point index) is
-// issued by one thread into buffer r % 2 once every warp has copied round
-// r - 2 from that buffer into registers (an mbarrier per buffer and
+// issued by one thread into buffer r % 2 as soon as every warp has copied
+// round r - 2 from that buffer into registers (an mbarrier per buffer and
 // direction: full after tcgen05.commit, empty after one arrival per warp);
 // warps meet at a CTA barrier only between cells. Every wait on an mbarrier
 // is bounded; a wait that runs out sets an error flag, the CTA stops taking
@@ -505,11 +505,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         // Round g (global count over the CTA's far cells) uses tensor-memory
         // buffer g & 1: full[b] completes when its MMAs are done (tcgen05.commit),
         // empty[b] when all 8 warps have read it into registers. Thread 0
-        // issues the cell's first two rounds at once and round g + 2 after it
-        // has evaluated round g (by then the other warps have almost always
-        // read round g, and the MMAs still have a whole round to finish);
-        // warps are not otherwise held together, so one warp's tensor-memory
-        // loads overlap the others' arithmetic.
+        // issues round g + 1 at the start of round g, after round g - 1's
+        // buffer is released; warps are not otherwise held together, so one
+        // warp's tensor-memory loads overlap the others' arithmetic.
         auto issue = [&](int g, int r) {  // thread 0 only: runtime indices are fine here
           const int a = r % kQ, ch = r / kQ, b = g & 1;
           bool fine = true;
@@ -530,7 +528,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           return fine;
         };
         bool ok = true;
-        if (tid == 0) ok = issue(g_round, 0) && issue(g_round + 1, 1);
+        if (tid == 0) ok = issue(g_round, 0);
         float2 slp[kQ], dlp[kQ];
 #pragma unroll
         for (int a = 0; a < kQ; ++a) {
@@ -544,6 +542,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
         for (int a = 0; a < kQ; ++a) {
           const int r = ch * kQ + a;
           const int g = g_round + r;
+          if (tid == 0 && r + 1 < kRounds) ok = issue(g + 1, r + 1) && ok;
           const int b = g & 1;
           ok = mbar_wait(mbar0 + 8 * b, (full_bits >> b) & 1u) && ok;
           full_bits ^= 1u << b;
@@ -578,7 +577,6 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           }
           slp[a] = __fadd2_rn(slp[a], sl2);
           dlp[a] = __fadd2_rn(dlp[a], dl2);
-          if (tid == 0 && r + 2 < kRounds) ok = issue(g + 2, r + 2) && ok;
         }
         }
         g_round += kRounds;
