@@ -32,13 +32,10 @@
 // Launch: one persistent CTA of 256 threads per SM (two warpgroups split
 // every 112-column chunk into halves of 56 columns), 512 tensor-memory
 // columns: two buffers x (d2, e) x 112. Round r = (chunk, point index) is
-// issued by one thread into buffer r % 2 as soon as every warp has copied
-// round r - 2 from that buffer into registers (an mbarrier per buffer and
-// direction: full after tcgen05.commit, empty after one arrival per warp);
-// warps meet at a CTA barrier only between cells. Every wait on an mbarrier
-// is bounded; a wait that runs out sets an error flag, the CTA stops taking
-// work, releases its tensor memory and exits, and the host reports
-// EB_ERR_TIMEOUT.
+// issued by one thread into buffer r % 2 while the threads evaluate round
+// r - 1. Every wait on an mbarrier is bounded; a wait that runs out sets an
+// error flag, the CTA stops taking work, releases its tensor memory and
+// exits, and the host reports EB_ERR_TIMEOUT.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -151,11 +148,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
     if (done) return true;
   }
   return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t mbar)
-{
-  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(mbar) : "memory");
 }
 
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -341,7 +333,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
 {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t s_mbar[4];  // full[2], empty[2]
+  __shared__ __align__(8) uint64_t s_mbar[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_item;
   __shared__ int s_stop;
@@ -366,10 +358,8 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    mbar_init(mbar0, 1);        // full[0]: one tcgen05.commit
-    mbar_init(mbar0 + 8, 1);    // full[1]
-    mbar_init(mbar0 + 16, kThreads / 32);  // empty[0]: one arrival per warp
-    mbar_init(mbar0 + 24, kThreads / 32);  // empty[1]
+    mbar_init(mbar0, 1);
+    mbar_init(mbar0 + 8, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_stop = 0;
   }
@@ -377,9 +367,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = s_tmem;
-  uint32_t full_bits = 0u;   // bit b: parity of the next completion of full[b]
-  uint32_t empty_bits = 0u;  // thread 0: parity of the next completion of empty[b]
-  int g_round = 0;           // far rounds this CTA has issued (buffer of round g: g & 1)
+  uint32_t phase_bits = 0u;  // bit b: parity of the next completion of mbarrier b
 
   for (;;) {
     if (tid == 0) s_item = s_stop ? nitems : atomicAdd(counter, 1);
@@ -502,21 +490,9 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           prefetched = cell + 1;
         }
         const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB), eBase = smem_u32(sE);
-        // Round g (global count over the CTA's far cells) uses tensor-memory
-        // buffer g & 1: full[b] completes when its MMAs are done (tcgen05.commit),
-        // empty[b] when all 8 warps have read it into registers. Thread 0
-        // issues round g + 1 at the start of round g, after round g - 1's
-        // buffer is released; warps are not otherwise held together, so one
-        // warp's tensor-memory loads overlap the others' arithmetic.
-        auto issue = [&](int g, int r) {  // thread 0 only: runtime indices are fine here
-          const int a = r % kQ, ch = r / kQ, b = g & 1;
-          bool fine = true;
-          if (g >= 2) {
-            fine = mbar_wait(mbar0 + 16 + 8 * b, (empty_bits >> b) & 1u);
-            empty_bits ^= 1u << b;
-            fence_after_sync();
-          }
-          const uint32_t d2 = tmem + (uint32_t)(b * 2 * kChunk);
+        auto issue = [&](int r) {
+          const int a = r % kQ, ch = r / kQ;  // thread 0 only: runtime indices are fine here
+          const uint32_t d2 = tmem + (uint32_t)((r & 1) * 2 * kChunk);
           const uint32_t de = d2 + kChunk;
 #pragma unroll
           for (int ks = 0; ks < 2; ++ks) {  // two K steps of 8 TF32
@@ -524,69 +500,68 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
             mma_tf32(d2, ad, umma_desc(bBase + ch * (kChunk / 8) * 512 + ks * 256), ks);
             mma_tf32(de, ad, umma_desc(eBase + ch * (kChunk / 8) * 512 + ks * 256), ks);
           }
-          mma_commit(mbar0 + 8 * b);
-          return fine;
+          mma_commit(mbar0 + 8 * (r & 1));
         };
-        bool ok = true;
-        if (tid == 0) ok = issue(g_round, 0);
+        if (tid == 0) issue(0);
         float2 slp[kQ], dlp[kQ];
 #pragma unroll
         for (int a = 0; a < kQ; ++a) {
           slp[a] = make_float2(0.f, 0.f);
           dlp[a] = make_float2(0.f, 0.f);
         }
-        const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+        bool ok = true;
 #pragma unroll 1
-        for (int ch = 0; ch < kChunks; ++ch) {
+        for (int ch = 0; ch < kChunks && ok; ++ch) {
 #pragma unroll
         for (int a = 0; a < kQ; ++a) {
           const int r = ch * kQ + a;
-          const int g = g_round + r;
-          if (tid == 0 && r + 1 < kRounds) ok = issue(g + 1, r + 1) && ok;
-          const int b = g & 1;
-          ok = mbar_wait(mbar0 + 8 * b, (full_bits >> b) & 1u) && ok;
-          full_bits ^= 1u << b;
+          if (tid == 0 && r + 1 < kRounds) issue(r + 1);
+          const int b = r & 1;
+          const bool waited = mbar_wait(mbar0 + 8 * b, (phase_bits >> b) & 1u);
+          phase_bits ^= 1u << b;
           fence_after_sync();
-          // the warpgroup's 56 columns of both products into registers at once
-          const uint32_t d2 = tmem + lane_base + (uint32_t)(b * 2 * kChunk + wg * kHalf);
+          const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
+          const uint32_t d2 = tmem + lane + (uint32_t)(b * 2 * kChunk + wg * kHalf);
           const uint32_t de = d2 + kChunk;
-          float vd[kHalf], ve[kHalf];
-#pragma unroll
-          for (int k = 0; k < kHalf / 8; ++k) {
-            tmem_ld8(d2 + 8 * k, vd + 8 * k);
-            tmem_ld8(de + 8 * k, ve + 8 * k);
-          }
-          tmem_wait_ld();
-          fence_before_sync();
-          __syncwarp();
-          if ((tid & 31) == 0) mbar_arrive(mbar0 + 16 + 8 * b);  // this warp is done with buffer b
           const float* cc2 = sC + ch * kChunk + wg * kHalf;
           float2 sl2 = make_float2(0.f, 0.f), dl2 = make_float2(0.f, 0.f);
+          // the warpgroup's 56 columns in blocks of 16, 16, 16 and 8
 #pragma unroll
-          for (int j = 0; j < kHalf; j += 4) {
-            const float4 c4 = *reinterpret_cast<const float4*>(cc2 + j);
+          for (int h0 = 0; h0 < kHalf; h0 += 16) {
+            constexpr int kMax = 16;
+            const int nb = (kHalf - h0) >= 16 ? 2 : 1;  // x8 blocks in this sub-chunk (compile-time after unrolling)
+            float vd[kMax], ve[kMax];
 #pragma unroll
-            for (int h = 0; h < 4; h += 2) {
-              const int jj = j + h;
-              const float2 cj = h == 0 ? make_float2(c4.x, c4.y) : make_float2(c4.z, c4.w);
-              const float2 ri = (jj % 16) >= 16 - kNewtonPer16 ? rsqrt2_newton(make_float2(vd[jj], vd[jj + 1]))
-                                                               : make_float2(rsq(vd[jj]), rsq(vd[jj + 1]));
+            for (int k = 0; k < 2; ++k)
+              if (k < nb) {
+                tmem_ld8(d2 + h0 + 8 * k, vd + 8 * k);
+                tmem_ld8(de + h0 + 8 * k, ve + 8 * k);
+              }
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < kMax; j += 2) {
+              if (j >= 8 * nb) break;
+              const float2 cj = *reinterpret_cast<const float2*>(cc2 + h0 + j);
+              const float2 ri = (j % 16) >= 16 - kNewtonPer16 ? rsqrt2_newton(make_float2(vd[j], vd[j + 1]))
+                                                              : make_float2(rsq(vd[j]), rsq(vd[j + 1]));
               sl2 = __ffma2_rn(cj, ri, sl2);
-              dl2 = __ffma2_rn(__fmul2_rn(ri, ri), __fmul2_rn(make_float2(ve[jj], ve[jj + 1]), ri), dl2);
+              dl2 = __ffma2_rn(__fmul2_rn(ri, ri), __fmul2_rn(make_float2(ve[j], ve[j + 1]), ri), dl2);
             }
           }
           slp[a] = __fadd2_rn(slp[a], sl2);
           dlp[a] = __fadd2_rn(dlp[a], dl2);
+          fence_before_sync();
+          ok = __syncthreads_and(waited) != 0;  // buffer b is free for round r + 2; same verdict in every thread
+          fence_after_sync();
+          if (!ok) break;
         }
         }
-        g_round += kRounds;
-        // every warp has read the cell's last round (so all its MMAs are
-        // done) before the operands are overwritten; same verdict everywhere
-        ok = __syncthreads_and(ok) != 0;
         if (!ok) {
           if (tid == 0) atomicExch(error_flag, 1);
           s_stop = 1;
           cp_async_wait_all();
+          // wait (bounded) for the MMAs already issued before the memory is released
+          for (int b = 0; b < 2; ++b) mbar_wait(mbar0 + 8 * b, (phase_bits >> b) & 1u);
           break;
         }
         if (active) {
