@@ -207,6 +207,12 @@ __device__ __forceinline__ void load_cell_operands(unsigned char* set, const Far
 #define EB_TC_NEWTON 0
 #endif
 constexpr int kNewtonPer16 = EB_TC_NEWTON;
+// Tensor-memory columns read per wait (a multiple of 8).
+#ifndef EB_TC_SUB
+#define EB_TC_SUB 16
+#endif
+constexpr int kSubCols = EB_TC_SUB;
+static_assert(kSubCols % 8 == 0 && kSubCols >= 8 && kSubCols <= 56, "tensor-memory read block");
 static_assert(kNewtonPer16 % 2 == 0 && kNewtonPer16 <= 16, "Newton columns come in pairs");
 
 // 1/sqrt(x) of two values on the FMA pipe: the magic-constant seed of the
@@ -525,14 +531,14 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           const uint32_t de = d2 + kChunk;
           const float* cc2 = sC + ch * kChunk + wg * kHalf;
           float2 sl2 = make_float2(0.f, 0.f), dl2 = make_float2(0.f, 0.f);
-          // the warpgroup's 56 columns in blocks of 16, 16, 16 and 8
+          // the warpgroup's 56 columns in blocks of kSubCols (the last one shorter)
 #pragma unroll
-          for (int h0 = 0; h0 < kHalf; h0 += 16) {
-            constexpr int kMax = 16;
-            const int nb = (kHalf - h0) >= 16 ? 2 : 1;  // x8 blocks in this sub-chunk (compile-time after unrolling)
+          for (int h0 = 0; h0 < kHalf; h0 += kSubCols) {
+            constexpr int kMax = kSubCols;
+            const int nb = min(kSubCols, kHalf - h0) / 8;  // x8 loads per product (compile-time after unrolling)
             float vd[kMax], ve[kMax];
 #pragma unroll
-            for (int k = 0; k < 2; ++k)
+            for (int k = 0; k < kMax / 8; ++k)
               if (k < nb) {
                 tmem_ld8(d2 + h0 + 8 * k, vd + 8 * k);
                 tmem_ld8(de + h0 + 8 * k, ve + 8 * k);
