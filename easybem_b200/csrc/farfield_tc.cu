@@ -67,7 +67,7 @@ static_assert(kTT == 128, "one tensor-memory lane per target triangle");
 // Source operands of the next well-separated cell of a work item are copied
 // into a second set of buffers (cp.async) while the current cell's rounds run.
 #ifndef EB_TC_PREFETCH
-#define EB_TC_PREFETCH 0
+#define EB_TC_PREFETCH 1  // measured: 159.7 -> 146.4 ms at L6
 #endif
 constexpr int kSets = EB_TC_PREFETCH ? 2 : 1;
 
@@ -204,7 +204,7 @@ __device__ __forceinline__ void load_cell_operands(unsigned char* set, const Far
 // instead of MUFU (MUFU is the tensor-core kernel's only saturated pipe; the
 // FMA pipe has half its time left).
 #ifndef EB_TC_NEWTON
-#define EB_TC_NEWTON 0
+#define EB_TC_NEWTON 2  // measured best of 0, 2, 4 (L6: 146.4, 141.1, 145.7 ms with the prefetch)
 #endif
 constexpr int kNewtonPer16 = EB_TC_NEWTON;
 // Tensor-memory columns read per wait (a multiple of 8).
