@@ -54,7 +54,7 @@ def test_separate_and_fused_applies_agree(gpu_lib, golden_ops):
         assert rel_l2(m.apply_dl(u), q) < 1e-14
 
 
-@pytest.mark.parametrize("level,nrows", [(4, 128), (6, 24)])
+@pytest.mark.parametrize("level,nrows", [(4, 128), (6, 24), (7, 16)])
 def test_large_mesh_sampled_rows_vs_oracle(gpu_lib, oracle, level, nrows):
     nodes, elems = meshes.perturbed_icosphere(level, seed=1)
     rng = np.random.default_rng(level)
