@@ -49,9 +49,12 @@ WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L{leve
 FMA_OPS_PER_PAIR = 8
 FLOPS_PER_PAIR = 2 * FMA_OPS_PER_PAIR
 RSQRT_PER_PAIR = 1
-# DRAM bytes (read + write) of one far-field launch on the L6 workload, from an ncu capture
-# of that launch (39.70 MB read + 1.36 MB written).
-FAR_TRAFFIC_L6 = 39.70e6 + 1.36e6
+# DRAM bytes (read + write) of one CUDA-core far-field launch on the L6 workload under the
+# plan of 512 work items per SM (the autotuner's choice there), from an ncu capture of that
+# launch: 46.61 MB read (records, target tables) + 110.48 MB written (the partial sums of
+# the 117-way source split).
+FAR_TRAFFIC_L6 = 46.61e6 + 110.48e6
+FAR_TRAFFIC_PLAN = 512
 
 
 def parse_args(argv=None):
@@ -288,7 +291,7 @@ def batch_record(local, solves=True):
         return a.elapsed_time(b) / k
 
     out = {}
-    for key, prec, engine in (("mixed", "mixed", "tensor"), ("mixed_cuda", "mixed", "cuda"), ("fp64", "fp64", "cuda")):
+    for key, prec, engine in (("mixed", "mixed", "cuda"), ("mixed_tensor", "mixed", "tensor"), ("fp64", "fp64", "cuda")):
         for m in ms:
             m.set_far_engine(engine)
         bt = eb.Batch(ms, precision=prec, sl_dl=True)
@@ -298,7 +301,7 @@ def batch_record(local, solves=True):
         out[key + "_vq"] = (torch.cat(d_v).cpu().numpy(), torch.cat(d_q).cpu().numpy())
         bt.close()
     for m in ms:
-        m.set_far_engine("tensor")
+        m.set_far_engine("cuda")
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     mixed_vs_fp64 = {"sl": rel(out["mixed_vq"][0], out["fp64_vq"][0]), "dl": rel(out["mixed_vq"][1], out["fp64_vq"][1])}
     # sampled rows of 8 meshes against the CPU oracle
@@ -327,9 +330,9 @@ def batch_record(local, solves=True):
     rec = {"workload": "256 ellipsoids (icosphere L2-L5, 320-20,480 triangles), SL+DL batched apply "
                        "(one density pair per mesh), 4-RHS SL batched apply, GMRES(50)-IR to 1e-8",
            "quad_pairs_per_apply": int(pairs), "mesh_setup_s": t_create,
-           "sl_dl_mixed": out["mixed"], "sl_dl_mixed_cuda_cores": out["mixed_cuda"], "sl_dl_fp64": out["fp64"],
+           "sl_dl_mixed": out["mixed"], "sl_dl_mixed_tensor_cores": out["mixed_tensor"], "sl_dl_fp64": out["fp64"],
            "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
-           "mixed_cuda_cores_over_fp64": out["mixed_cuda"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
+           "mixed_tensor_cores_over_fp64": out["mixed_tensor"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "rel_err_vs_oracle": err,
            "sl_4rhs_mixed": {"ms_per_apply": ms4, "Gpairs_per_s": pairs / (ms4 * 1e-3) / 1e9,
                              "rhs_evals_per_s_G": 4 * pairs / (ms4 * 1e-3) / 1e9}}
@@ -382,26 +385,27 @@ def large_record(local, solve=False):
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     pairs = m.far_quad_pairs
     peak_tflops, peak_rsqrt = _measure_peak()
-    rate = pairs / (res["mixed"][2] * 1e-3)
+    rate_t = pairs / (res["mixed"][2] * 1e-3)  # tensor-core engine
     mufu_pp, fma_pp, _ = _engine_costs("tensor")
-    bound = min(peak_tflops * 1e12 / (2 * fma_pp), peak_rsqrt * 1e12 / mufu_pp)
-    rate_c = pairs / (res["mixed_cuda"][2] * 1e-3)
-    bound_c = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
+    bound_t = min(peak_tflops * 1e12 / (2 * fma_pp), peak_rsqrt * 1e12 / mufu_pp)
+    rate = pairs / (res["mixed_cuda"][2] * 1e-3)  # CUDA cores: the default engine
+    bound = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
     cf, cn = m.cell_pairs()
     rec = {"workload": "radius-perturbed icosphere L7 (327,680 triangles, 163,842 vertices)",
            "quad_pairs_per_step": pairs, "near_pairs": m.near_pairs, "mesh_setup_s": t_create,
            "near_cell_share": cn / (cf + cn),
-           "mixed": {"engine": "tensor", "far_ms": res["mixed"][2], "finalize_ms": res["mixed"][3],
-                     "Gpairs_per_s": rate / 1e9, "mufu_frac": rate * mufu_pp / (peak_rsqrt * 1e12),
+           "mixed": {"engine": "cuda", "far_ms": res["mixed_cuda"][2], "finalize_ms": res["mixed_cuda"][3],
+                     "Gpairs_per_s": rate / 1e9, "fma_pipe_frac": rate * FLOPS_PER_PAIR / (peak_tflops * 1e12),
                      "frac_of_pair_bound": rate / bound},
-           "mixed_cuda_cores": {"far_ms": res["mixed_cuda"][2], "Gpairs_per_s": rate_c / 1e9,
-                                "fma_pipe_frac": rate_c * FLOPS_PER_PAIR / (peak_tflops * 1e12),
-                                "frac_of_pair_bound": rate_c / bound_c,
-                                "rel_err_sl": rel(res["mixed_cuda"][0][rows], vo),
-                                "rel_err_dl": rel(res["mixed_cuda"][1][rows], qo)},
+           "mixed_tensor_cores": {"far_ms": res["mixed"][2], "Gpairs_per_s": rate_t / 1e9,
+                                  "mufu_frac": rate_t * mufu_pp / (peak_rsqrt * 1e12),
+                                  "frac_of_pair_bound": rate_t / bound_t,
+                                  "rel_err_sl": rel(res["mixed"][0][rows], vo),
+                                  "rel_err_dl": rel(res["mixed"][1][rows], qo)},
            "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
                     "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
-           "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed"][0][rows], vo), "mixed_dl": rel(res["mixed"][1][rows], qo),
+           "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed_cuda"][0][rows], vo),
+                                 "mixed_dl": rel(res["mixed_cuda"][1][rows], qo),
                                  "fp64_sl": rel(res["fp64"][0][rows], vo), "fp64_dl": rel(res["fp64"][1][rows], qo),
                                  "oracle_rows": len(rows)}}
     rec["mixed_over_fp64"] = rec["mixed"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
@@ -657,7 +661,8 @@ def main():
                                if args.far_engine == "tensor" else "FMA pipe and MUFU together"),
                      "achieved": pair_rate / 1e9, "peak": pair_bound / 1e9, "unit": "Gpairs/s",
                      "frac": pair_rate / pair_bound,
-                     "traffic": FAR_TRAFFIC_L6 if (args.level == LEVEL and args.far_engine == "cuda") else None,
+                     "traffic": FAR_TRAFFIC_L6 if (args.level == LEVEL and args.far_engine == "cuda"
+                                                   and plan_info.get("items_per_sm") == FAR_TRAFFIC_PLAN) else None,
                      "traffic_unit": "bytes per launch",
                      "kernel": "far_tc_kernel" if args.far_engine == "tensor" else "far_kernel<float,7,7,1,true>",
                      "far_ms": far_avg,
