@@ -24,7 +24,6 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
   constexpr int NS = NSL > 0 ? NSL : 1;
   constexpr int NACC = P1T ? 3 : NS + NDX;
   static_assert(!P1T || (NSL == 1 && !DL), "P1 test functions pair with one SL charge");
-  constexpr bool kDup = kDupRecords && F32 && NSL == 1 && ND == 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_item;
   __shared__ int4 s_vid[kTS];
@@ -82,19 +81,8 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
     for (int t0 = sb; t0 < se; t0 += ts) {
       const int ns = min(ts, se - t0);
       const S* g = grec + (size_t)t0 * nq * NREC;
-      if constexpr (kDup) {  // (v, v) pairs: three float4 per source point
-        const float4* gf = reinterpret_cast<const float4*>(g);
-        float4* sf4 = reinterpret_cast<float4*>(s_rec);
-        for (int k = threadIdx.x; k < ns * nq; k += kTT) {
-          const float4 a = gf[2 * k], c = gf[2 * k + 1];  // (-2y, |y|^2), (s, c, 0, 0)
-          sf4[3 * k] = make_float4(a.x, a.x, a.y, a.y);
-          sf4[3 * k + 1] = make_float4(a.z, a.z, a.w, a.w);
-          sf4[3 * k + 2] = make_float4(c.y, c.y, c.x, c.x);
-        }
-      } else {
-        const int nslot = ns * nq * NREC;
-        for (int k = threadIdx.x; k < nslot; k += kTT) s_rec[k] = g[k];
-      }
+      const int nslot = ns * nq * NREC;
+      for (int k = threadIdx.x; k < nslot; k += kTT) s_rec[k] = g[k];
       for (int k = threadIdx.x; k < ns; k += kTT) {
         s_vid[k] = md.svid[t0 + k];
         if constexpr (DL) {
@@ -134,11 +122,11 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
           if constexpr (F32) {
             const float* sf = reinterpret_cast<const float*>(s_rec);
             if (far)
-              eval_cell_x2<K, NQ, NSL, ND, true, kDup>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
-                                                       cen, nrm, sl, dl);
+              eval_cell_x2<K, NQ, NSL, ND, true>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+                                                 nrm, sl, dl);
             else
-              eval_cell_x2<K, NQ, NSL, ND, false, kDup>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,
-                                                        cen, nrm, sl, dl);
+              eval_cell_x2<K, NQ, NSL, ND, false>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+                                                  nrm, sl, dl);
           } else {
             if (far)
               eval_cell<T, K, NQ, NSL, ND, true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o,

@@ -37,18 +37,11 @@ constexpr int kTT = EB_TT;  // target items (threads) per CTA
 constexpr int kTS = 64;   // source triangles per shared-memory tile (Q <= 7)
 constexpr int kMaxRecSlots = 3;  // record slots of the widest variant
 constexpr int kMaxOutputs = 5;   // SL charges + DL of the widest variant
-// The FP32 far kernel of the fused SL+DL variant stages its source records
-// with every value duplicated ((v, v) operand pairs for FFMA2): 3 slots of
-// 16 bytes per point instead of 2.
-#ifndef EB_X2_DUP
-#define EB_X2_DUP 0
-#endif
-constexpr bool kDupRecords = EB_X2_DUP != 0;
 // Shared memory of a staged source tile: 16 bytes per FP32 record slot,
-// 32 per FP64 slot (FP32 two-slot variants: room for the duplicated form).
+// 32 per FP64 slot.
 __host__ __device__ constexpr size_t far_smem_bytes(int src_tile, int Q, int nrec, bool fp32)
 {
-  return (size_t)src_tile * Q * (fp32 && kDupRecords && nrec == 2 ? 3 : nrec) * (fp32 ? 16 : 32);
+  return (size_t)src_tile * Q * nrec * (fp32 ? 16 : 32);
 }
 constexpr int kPrepBlock = 256;     // threads per block of the record preparation (one source point each)
 constexpr int kFinalizeBlock = 128; // threads per block of the finalize

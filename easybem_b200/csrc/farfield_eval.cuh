@@ -193,11 +193,7 @@ __device__ __forceinline__ void eval_cell(const typename Slot<T>::type* __restri
 // FMA-pipe work per quadrature pair is unchanged (FFMA2 occupies the pipe
 // for two lanes' worth); the pair form halves the issue slots, which bound
 // the scalar loop.
-// DUP: the staged records of the fused SL+DL variant hold every source value
-// twice, (v, v), so that a 128-bit shared load yields ready operand pairs:
-// three float4 per source point, ((-2y)_x (-2y)_x (-2y)_y (-2y)_y),
-// ((-2y)_z (-2y)_z |y|^2 |y|^2), (c c s s).
-template <int K, int NQ, int NSL, int ND, bool FAR, bool DUP = false>
+template <int K, int NQ, int NSL, int ND, bool FAR>
 __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, const int4* __restrict__ svid,
                                              const dq* __restrict__ snrm, const float4* __restrict__ splane, int s0,
                                              int s1, int nq, int4 tv, const float (&x)[K], const float (&y)[K],
@@ -212,8 +208,7 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
   constexpr int KP = K / 2;           // packed target pairs
   constexpr int KP1 = KP > 0 ? KP : 1;
   constexpr bool ODD = (K & 1) != 0;  // last target point runs scalar
-  static_assert(!DUP || (NSL == 1 && ND == 1), "duplicated records: fused SL+DL variant only");
-  constexpr int PS = DUP ? 12 : 4 * NREC;  // staged floats per source point
+  constexpr int PS = 4 * NREC;        // staged floats per source point
   const int nqr = NQ > 0 ? NQ : nq;
   float2 X[KP1], Y[KP1], Z[KP1], W[KP1], SL[NS][KP1], DLp[NDX][KP1];
 #pragma unroll
@@ -246,27 +241,20 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
     for (int b = 0; b < nqr; ++b) {
       const float* rb = r + b * PS;
       const float4* rv = reinterpret_cast<const float4*>(rb);
-      float2 px, py, pz, pw, ch[NS], sd[NDX];
-      if constexpr (DUP) {
-        const float4 q0 = rv[0], q1 = rv[1], q2 = rv[2];
-        px = make_float2(q0.x, q0.y); py = make_float2(q0.z, q0.w);
-        pz = make_float2(q1.x, q1.y); pw = make_float2(q1.z, q1.w);
-        ch[0] = make_float2(q2.x, q2.y);
-        sd[0] = make_float2(q2.z, q2.w);
-      } else {
-        const float4 p0 = rv[0];
-        px = make_float2(p0.x, p0.x); py = make_float2(p0.y, p0.y);
-        pz = make_float2(p0.z, p0.z); pw = make_float2(p0.w, p0.w);
+      const float4 p0 = rv[0];
+      const float2 px = make_float2(p0.x, p0.x), py = make_float2(p0.y, p0.y);
+      const float2 pz = make_float2(p0.z, p0.z), pw = make_float2(p0.w, p0.w);
+      float2 ch[NS];
 #pragma unroll
-        for (int c = 0; c < NSL; ++c) {
-          const float v = comp(rv[charge_slot(c, ND)], charge_comp(c, ND));
-          ch[c] = make_float2(v, v);
-        }
+      for (int c = 0; c < NSL; ++c) {
+        const float v = comp(rv[charge_slot(c, ND)], charge_comp(c, ND));
+        ch[c] = make_float2(v, v);
+      }
+      float2 sd[NDX];
 #pragma unroll
-        for (int c = 0; c < NDX; ++c) {
-          const float v = DL ? comp(rv[1], c) : 0.f;
-          sd[c] = make_float2(v, v);
-        }
+      for (int c = 0; c < NDX; ++c) {
+        const float v = DL ? comp(rv[1], c) : 0.f;
+        sd[c] = make_float2(v, v);
       }
 #pragma unroll
       for (int p = 0; p < KP; ++p) {
