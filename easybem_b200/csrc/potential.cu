@@ -84,7 +84,7 @@ __device__ __forceinline__ double pot_rsq(double x) { return rsqrt(x); }
 // records: 2 slots per source point, slot0 = (-2 y_rel, |y_rel|^2), slot1 = (s, c, ., .)
 template <typename T>
 __global__ void __launch_bounds__(kPotThreads) potential_kernel(int npts, const double* __restrict__ pts, int ne,
-                                                                int Q, int cells_per_chunk,
+                                                                int Q, int cells_per_chunk, int ts,
                                                                 const typename PotSlot<T>::type* __restrict__ rec,
                                                                 const typename PotSlot<T>::type* __restrict__ plane,
                                                                 const dq* __restrict__ ccent,
@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(kPotThreads) potential_kernel(int npts, const 
   const int c0 = blockIdx.y * cells_per_chunk, c1 = min(ncells, c0 + cells_per_chunk);
   const int sb = c0 * kCell, se = min(ne, c1 * kCell);
   T hi = 0, lo = 0;
-  for (int t0 = sb; t0 < se; t0 += kTS) {
-    const int ns = min(kTS, se - t0);
+  for (int t0 = sb; t0 < se; t0 += ts) {  // ts <= kTS source triangles per staged tile
+    const int ns = min(ts, se - t0);
     for (int k = threadIdx.x; k < ns * Q * 2; k += kPotThreads) s_rec[k] = rec[(size_t)t0 * Q * 2 + k];
     for (int k = threadIdx.x; k < ns; k += kPotThreads) s_plane[k] = plane[t0 + k];
     __syncthreads();
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kPotThreads) potential_kernel(int npts, const 
 // with packed FFMA2/FMUL2, every source value broadcast to both halves; the
 // arithmetic per lane is that of the scalar kernel above.
 __global__ void __launch_bounds__(kPotThreads) potential_x2_kernel(int npts, const double* __restrict__ pts, int ne,
-                                                                   int Q, int cells_per_chunk,
+                                                                   int Q, int cells_per_chunk, int ts,
                                                                    const float4* __restrict__ rec,
                                                                    const float4* __restrict__ plane,
                                                                    const dq* __restrict__ ccent,
@@ -165,8 +165,8 @@ __global__ void __launch_bounds__(kPotThreads) potential_x2_kernel(int npts, con
   const float2 half2 = make_float2(0.5f, 0.5f);
   float hi[2] = {0.f, 0.f}, lo[2] = {0.f, 0.f};
   double near[2] = {0.0, 0.0};  // FP64 sums of the cells close to each point
-  for (int t0 = sb; t0 < se; t0 += kTS) {
-    const int ns = min(kTS, se - t0);
+  for (int t0 = sb; t0 < se; t0 += ts) {  // ts <= kTS source triangles per staged tile
+    const int ns = min(ts, se - t0);
     for (int k = threadIdx.x; k < ns * Q * 2; k += kPotThreads) s_rec[k] = rec[(size_t)t0 * Q * 2 + k];
     for (int k = threadIdx.x; k < ns; k += kPotThreads) s_plane[k] = plane[t0 + k];
     __syncthreads();
@@ -234,7 +234,6 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
   if (precision != EB_PREC_MIXED && precision != EB_PREC_FP64)
     return set_error(EB_ERR_INVALID, "precision must be EB_PREC_FP64 or EB_PREC_MIXED");
   if (npts < 1) return EB_OK;
-  if (h.Q > 16) return set_error(EB_ERR_INVALID, "potential evaluation supports triangle rules of up to 16 points");
   // source records of the fused SL+DL variant (slot1 = (s, c))
   if (!m->rec.p) {
     EB_CHECK(m->rec.alloc((size_t)h.ne * h.Q * kMaxRecSlots * sizeof(dq)));
@@ -255,18 +254,22 @@ int mesh_evaluate_potential(Mesh* m, int precision, int npts, const double* d_pt
   const int cells_per = (h.ncells + nchunk - 1) / nchunk;
   nchunk = (h.ncells + cells_per - 1) / cells_per;
   EB_CHECK(m->pot_partial.alloc(sizeof(double) * (size_t)nchunk * npts));
-  const size_t smem = (size_t)kTS * h.Q * 2 * (fp32 ? sizeof(float4) : sizeof(dq));
+  // source triangles per staged tile: whole cells' worth up to kTS, fewer
+  // for large rules so the tile stays within 48 KB of shared memory
+  const size_t per_tri = (size_t)h.Q * 2 * (fp32 ? sizeof(float4) : sizeof(dq));
+  const int ts = (int)std::max<size_t>(1, std::min<size_t>(kTS, (48 * 1024) / per_tri));
+  const size_t smem = (size_t)ts * per_tri;
   const dim3 grid(pblocks, nchunk);
   if (fp32) {
     auto k = potential_x2_kernel;
     if (smem > 32 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, m->rec.as<float4>(),
+    k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, ts, m->rec.as<float4>(),
                                        m->splane32.as<float4>(), m->ccent.as<dq>(), m->pot_rec64.as<dq>(),
                                        m->splane64.as<dq>(), m->pot_partial.as<double>());
   } else {
     auto k = potential_kernel<double>;
     if (smem > 32 * 1024) EB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, m->rec.as<dq>(), m->splane64.as<dq>(),
+    k<<<grid, kPotThreads, smem, st>>>(npts, d_pts, h.ne, h.Q, cells_per, ts, m->rec.as<dq>(), m->splane64.as<dq>(),
                                        m->ccent.as<dq>(), m->pot_partial.as<double>());
   }
   EB_CUDA(cudaGetLastError());

@@ -131,7 +131,7 @@ int eb_apply_hypersingular_device(eb_mesh mesh, int precision, const double* d_u
                                   void* stream);
 
 /* u(x) = V t - W u at npts points off the surface (the representation formula
- * with the triangle rule of the mesh's order, up to 16 points): pts [npts][3],
+ * with the triangle rule of the mesh's order, any index): pts [npts][3],
  * t [nelems], u [nnodes], out [npts], host memory. Replaces evaluateLaplace3d
  * (src/BEM3dLaplace.cpp:784-843). */
 int eb_evaluate_potential(eb_mesh mesh, int precision, int npts, const double* pts, const double* t,

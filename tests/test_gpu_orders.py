@@ -58,3 +58,25 @@ def test_hypersingular_on_the_neumann_driver_mesh(gpu_lib, golden_orders):
     with gpu_lib.Mesh(nodes, elems, 4) as m:
         assert rel_l2(m.apply_hypersingular(u), z["shaft1_o4_Du"]) < 1e-11
         assert rel_l2(m.apply_hypersingular(u, precision="mixed"), z["shaft1_o4_Du"]) < MIXED_TOL
+
+
+@pytest.mark.parametrize("order", [9, 13, 18])
+def test_potential_at_large_rules(gpu_lib, golden_orders, oracle, order):
+    """evaluateLaplace3d (src/BEM3dLaplace.cpp:784-843) at the reference
+    driver's indices on its shaft mesh (25- to 73-point rules), points inside,
+    outside and within a fraction of an element of the surface, against the
+    oracle (pinned to the reference's evaluateLaplace3d on CPU)."""
+    z = golden_orders
+    nodes, elems, t, u = z["shaft0_nodes"], z["shaft0_elems"], z["shaft0_t"], z["shaft0_u"]
+    c = nodes.mean(axis=0)
+    rng = np.random.default_rng(order)
+    tri = nodes[elems[rng.choice(elems.shape[0], 40)] - 1].mean(axis=1)
+    n = rng.normal(size=(40, 3))
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    pts = np.vstack([tri + 0.02 * n, c + rng.normal(size=(20, 3)) * 0.3, c + rng.normal(size=(20, 3)) * 4.0])
+    oracle.set_order(order)
+    ref = oracle.evaluate(nodes, elems, pts, t, u)
+    oracle.set_order(4)
+    with gpu_lib.Mesh(nodes, elems, order) as m:
+        assert rel_l2(m.evaluate(pts, t, u), ref) < 1e-12
+        assert rel_l2(m.evaluate(pts, t, u, precision="mixed"), ref) < MIXED_TOL

@@ -228,3 +228,20 @@ def test_p1_singular_pairs_converge_and_swap_symmetrically(oracle):
         print(f"P1 pair ({i},{j}): max relative change to index 18 at indices 6/10/14/16: {errs}")
         assert errs[-1] <= 1e-10 and errs[0] > errs[-1], (i, j, errs)
     oracle.set_order(4)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+def test_oracle_potential_matches_reference_at_large_rules(oracle):
+    """The port's evaluateLaplace3d against the reference's own at indices 13
+    and 18 on a perturbed sphere."""
+    nodes, elems = meshes.perturbed_icosphere(1, seed=4)
+    rng = np.random.default_rng(2)
+    t = rng.normal(size=elems.shape[0])
+    u = rng.normal(size=nodes.shape[0])
+    pts = rng.normal(size=(30, 3)) * np.array([0.5, 0.5, 2.5])[None, :]
+    for order in (13, 18):
+        oracle.set_order(order)
+        got = oracle.evaluate(nodes, elems, pts, t, u)
+        ref = O.ref_evaluate(nodes, elems, pts, t, u, order)
+        assert rel_l2(got, ref) < 1e-13, order
+    oracle.set_order(4)
