@@ -80,3 +80,17 @@ def test_potential_at_large_rules(gpu_lib, golden_orders, oracle, order):
     with gpu_lib.Mesh(nodes, elems, order) as m:
         assert rel_l2(m.evaluate(pts, t, u), ref) < 1e-12
         assert rel_l2(m.evaluate(pts, t, u, precision="mixed"), ref) < MIXED_TOL
+
+
+def test_p1_single_layer_at_a_large_rule(gpu_lib, golden_orders, oracle):
+    """applyGPULaplace3d1Layer(t, v, 1) (P1 x P1) at index 10 (25-point
+    triangle rule, 12-point line rule) on the reference driver's shaft mesh,
+    against the oracle's dense P1 matrix at the same index."""
+    z = golden_orders
+    nodes, elems, u = z["shaft0_nodes"], z["shaft0_elems"], z["shaft0_u"]
+    oracle.set_order(10)
+    ref = oracle.p1_dense(nodes, elems) @ u
+    oracle.set_order(4)
+    with gpu_lib.Mesh(nodes, elems, 10) as m:
+        assert rel_l2(m.apply_sl_p1(u), ref) < 1e-12
+        assert rel_l2(m.apply_sl_p1(u, precision="mixed"), ref) < MIXED_TOL
