@@ -212,6 +212,11 @@ constexpr int kNewtonPer16 = EB_TC_NEWTON;
 #define EB_TC_SUB 16
 #endif
 constexpr int kSubCols = EB_TC_SUB;
+// Independent accumulators per product and thread within a round.
+#ifndef EB_TC_ACC
+#define EB_TC_ACC 1
+#endif
+constexpr int kAcc = EB_TC_ACC;
 static_assert(kSubCols % 8 == 0 && kSubCols >= 8 && kSubCols <= 56, "tensor-memory read block");
 static_assert(kNewtonPer16 % 2 == 0 && kNewtonPer16 <= 16, "Newton columns come in pairs");
 
@@ -530,7 +535,11 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
           const uint32_t d2 = tmem + lane + (uint32_t)(b * 2 * kChunk + wg * kHalf);
           const uint32_t de = d2 + kChunk;
           const float* cc2 = sC + ch * kChunk + wg * kHalf;
-          float2 sl2 = make_float2(0.f, 0.f), dl2 = make_float2(0.f, 0.f);
+          // kAcc independent accumulator pairs per product (column pairs taken
+          // round-robin) so consecutive FFMA2s do not wait on each other
+          float2 sl2[kAcc], dl2[kAcc];
+#pragma unroll
+          for (int k = 0; k < kAcc; ++k) sl2[k] = dl2[k] = make_float2(0.f, 0.f);
           // the warpgroup's 56 columns in blocks of kSubCols (the last one shorter)
 #pragma unroll
           for (int h0 = 0; h0 < kHalf; h0 += kSubCols) {
@@ -550,12 +559,16 @@ __global__ void __launch_bounds__(tc::kThreads, 1)
               const float2 cj = *reinterpret_cast<const float2*>(cc2 + h0 + j);
               const float2 ri = (j % 16) >= 16 - kNewtonPer16 ? rsqrt2_newton(make_float2(vd[j], vd[j + 1]))
                                                               : make_float2(rsq(vd[j]), rsq(vd[j + 1]));
-              sl2 = __ffma2_rn(cj, ri, sl2);
-              dl2 = __ffma2_rn(__fmul2_rn(ri, ri), __fmul2_rn(make_float2(ve[j], ve[j + 1]), ri), dl2);
+              const int k = ((h0 + j) / 2) % kAcc;
+              sl2[k] = __ffma2_rn(cj, ri, sl2[k]);
+              dl2[k] = __ffma2_rn(__fmul2_rn(ri, ri), __fmul2_rn(make_float2(ve[j], ve[j + 1]), ri), dl2[k]);
             }
           }
-          slp[a] = __fadd2_rn(slp[a], sl2);
-          dlp[a] = __fadd2_rn(dlp[a], dl2);
+#pragma unroll
+          for (int k = 0; k < kAcc; ++k) {
+            slp[a] = __fadd2_rn(slp[a], sl2[k]);
+            dlp[a] = __fadd2_rn(dlp[a], dl2[k]);
+          }
           fence_before_sync();
           ok = __syncthreads_and(waited) != 0;  // buffer b is free for round r + 2; same verdict in every thread
           fence_after_sync();
