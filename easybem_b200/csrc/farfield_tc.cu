@@ -214,7 +214,7 @@ constexpr int kNewtonPer16 = EB_TC_NEWTON;
 constexpr int kSubCols = EB_TC_SUB;
 // Independent accumulators per product and thread within a round.
 #ifndef EB_TC_ACC
-#define EB_TC_ACC 1
+#define EB_TC_ACC 1  // measured best of 1, 2, 4 (L6: 138.3, 141.3, 144.5 ms)
 #endif
 constexpr int kAcc = EB_TC_ACC;
 static_assert(kSubCols % 8 == 0 && kSubCols >= 8 && kSubCols <= 56, "tensor-memory read block");
