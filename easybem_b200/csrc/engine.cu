@@ -636,6 +636,8 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
   desc.nsplit = m->plan.nsplit;
   desc.src_tile = src_tile_for(h.Q, fp32, nsl, nd);
   if (m->plan.tile > 0) desc.src_tile = std::min(desc.src_tile, m->plan.tile);
+  // the FP32 far kernel stages source triangles in pairs
+  if (fp32) desc.src_tile = std::max(2, desc.src_tile & ~1);
   desc.active = nullptr;
   return desc;
 }

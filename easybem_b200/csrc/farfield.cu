@@ -9,15 +9,46 @@
 
 namespace eb {
 
+// Shape of the FP32 far kernel per variant. far_source_pairs: eval_cell_sp over
+// a source-pair tile, or eval_cell_x2 (target points in pairs) for the
+// variants with three or more SL charges unless EB_SP_WIDE, and for the
+// 8-point four-column DL variant, whose packed sums would spill.
+// far_min_blocks: resident CTAs per SM the registers are capped for; the
+// one-output variants (SL, P1-tested SL, DL up to 7 points) fit 3 without
+// spills, as do the wide SL variants in the target-pair form.
+#ifndef EB_SP_WIDE
+#define EB_SP_WIDE 1
+#endif
+#ifndef EB_MINB_NARROW
+#define EB_MINB_NARROW EB_F32_MINB
+#endif
+#ifndef EB_MINB_WIDE
+#define EB_MINB_WIDE EB_F32_MINB
+#endif
+template <typename T, int K, int NSL, int ND>
+__host__ __device__ constexpr bool far_source_pairs()
+{
+  return std::is_same<T, float>::value && kFarSourcePairs && !(K >= 8 && ND >= 4) && (NSL < 3 || EB_SP_WIDE);
+}
+template <typename T, int K, int NSL, int ND>
+__host__ __device__ constexpr int far_min_blocks()
+{
+  return !std::is_same<T, float>::value     ? EB_F64_MINB
+         : NSL + ND == 1 && (NSL || K < 8) ? EB_MINB_NARROW
+         : NSL >= 3                         ? EB_MINB_WIDE
+                                            : EB_F32_MINB;
+}
+
 // P1T: P1 test functions; the item's three outputs are sum_a w_a phi_k(x_a) acc_a
 // (k = 0, 1, 2 in the triangle's vertex order) of the single SL charge.
 template <typename T, int K, int NQ, int NSL, int ND, bool P1T>
-__global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MINB : EB_F64_MINB)
+__global__ void __launch_bounds__(kTT, far_min_blocks<T, K, NSL, ND>())
     far_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
                int* __restrict__ counter)
 {
   using S = typename Slot<T>::type;
   constexpr bool F32 = std::is_same<T, float>::value;
+  constexpr bool SP = far_source_pairs<T, K, NSL, ND>();
   constexpr bool DL = ND > 0;
   constexpr int NDX = ND > 0 ? ND : 1;
   constexpr int NREC = rec_slots(NSL, ND);
@@ -76,13 +107,36 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
 
     const int sb = w.cell0 * kCell;
     const int se = min(md.ne, w.cell1 * kCell);
-    const int ts = md.src_tile;
+    // FP32 tiles pair their triangles (an even tile size, at least 2, set by the host)
+    const int ts = SP ? (md.src_tile & ~1) : md.src_tile;
     const S* grec = reinterpret_cast<const S*>(md.rec);
     for (int t0 = sb; t0 < se; t0 += ts) {
       const int ns = min(ts, se - t0);
       const S* g = grec + (size_t)t0 * nq * NREC;
-      const int nslot = ns * nq * NREC;
-      for (int k = threadIdx.x; k < nslot; k += kTT) s_rec[k] = g[k];
+      if constexpr (SP) {
+        // source-pair layout: record slot (2p, b, k) and (2p+1, b, k) interleaved
+        const int per = nq * NREC;
+        const int nstage = ((ns + 1) >> 1) * per;
+        for (int k = threadIdx.x; k < nstage; k += kTT) {
+          const int p = k / per, rem = k - p * per;
+          const S a = g[(size_t)(2 * p) * per + rem];
+          S c;
+          if (2 * p + 1 < ns) c = g[(size_t)(2 * p + 1) * per + rem];
+          else c = rem % NREC == 0 ? make_float4(0.f, 0.f, 0.f, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+          s_rec[2 * k] = make_float4(a.x, c.x, a.y, c.y);
+          s_rec[2 * k + 1] = make_float4(a.z, c.z, a.w, c.w);
+        }
+        if ((ns & 1) && threadIdx.x == 0) {
+          s_vid[ns] = make_int4(-1, -1, -1, 0);
+          if constexpr (DL) {
+            s_nrm[ns] = dq{0.0, 0.0, 0.0, 0.0};
+            s_plane[ns] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+      } else {
+        const int nslot = ns * nq * NREC;
+        for (int k = threadIdx.x; k < nslot; k += kTT) s_rec[k] = g[k];
+      }
       for (int k = threadIdx.x; k < ns; k += kTT) {
         s_vid[k] = md.svid[t0 + k];
         if constexpr (DL) {
@@ -119,7 +173,14 @@ __global__ void __launch_bounds__(kTT, std::is_same<T, float>::value ? EB_F32_MI
 #pragma unroll
             for (int c = 0; c < NS; ++c) sl[c][a] = 0;
           }
-          if constexpr (F32) {
+          if constexpr (SP) {
+            if (far)
+              eval_cell_sp<K, NQ, NSL, ND, true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+                                                 nrm, sl, dl);
+            else
+              eval_cell_sp<K, NQ, NSL, ND, false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,
+                                                  nrm, sl, dl);
+          } else if constexpr (F32) {
             const float* sf = reinterpret_cast<const float*>(s_rec);
             if (far)
               eval_cell_x2<K, NQ, NSL, ND, true>(sf, s_vid, s_nrm, s_plane, g0, g1, nq, tv, xs, ys, zs, q2, o, cen,

@@ -28,7 +28,10 @@
 #define EB_UNROLL_WIDE_F64 1  // FP64 variants with three or more outputs
 #endif
 #ifndef EB_UNROLL_B_X2
-#define EB_UNROLL_B_X2 0  // source-point unroll of the packed FP32 form (0: full)
+#define EB_UNROLL_B_X2 0  // source-point unroll of the packed FP32 forms (0: full)
+#endif
+#ifndef EB_FAR_SP
+#define EB_FAR_SP 1  // FP32 far kernel: 1 pairs source triangles (eval_cell_sp), 0 pairs target points (eval_cell_x2)
 #endif
 
 namespace eb {
@@ -36,6 +39,7 @@ namespace eb {
 constexpr int kUnrollF32 = EB_UNROLL_B_F32;
 constexpr int kUnrollF64 = EB_UNROLL_B_F64;
 constexpr int kUnrollX2 = EB_UNROLL_B_X2;
+constexpr bool kFarSourcePairs = EB_FAR_SP != 0;
 
 // Neumann/Knuth two-sum accumulation: (s, e) holds s + e exactly up to the
 // rounding of e.
@@ -338,6 +342,147 @@ __device__ __forceinline__ void eval_cell_x2(const float* __restrict__ srec, con
       dl[c][2 * p] += DLp[c][p].x;
       dl[c][2 * p + 1] += DLp[c][p].y;
     }
+  }
+}
+
+// Source-pair layout of a staged FP32 tile: triangles 2p and 2p+1 of the tile
+// share one record of 2 * NREC float4 per quadrature point, in which record
+// slot k occupies float4 2k and 2k+1 as (c0, c0', c1, c1') and (c2, c2', c3,
+// c3') (unprimed: triangle 2p, primed: 2p+1). An odd last triangle is paired
+// with a zero-strength dummy at (-2y, |y|^2) = (0, 0, 0, 1). Component c of
+// slot k of both triangles, as one FFMA2 operand:
+__device__ __forceinline__ float2 sp_comp(const float4* rv, int slot, int c)
+{
+  const float4 v = rv[2 * slot + (c >> 1)];
+  return (c & 1) ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+}
+
+// eval_cell over a source-pair tile: the two lanes of every FFMA2 are the same
+// target point against the same quadrature point of triangles s and s+1, so
+// each target value is broadcast once per cell (not per source point), each
+// LDS.128 lands in aligned register pairs, and every target point runs packed.
+// Per lane the arithmetic and its rounding are those of eval_cell_x2 (far
+// cells: expanded |x - y|^2; other cells: direct differences); the SL and DL
+// sums of the two lanes are added per cell. Other cells mask a lane whose
+// triangle shares a vertex with the target by zeroing its strengths, and add
+// 1e-24 to |x - y|^2 so the target triangle's own (zero-strength) points give
+// 0 * finite: 1/r = 1e12 and 1/r^3 = 1e36 stay below the FP32 maximum, and the
+// term changes no squared distance above 1.7e-17 (points 4e-9 apart). s0 is
+// even; s1 - s0 may be odd at the end of the mesh, where the staged dummy
+// completes the last pair.
+template <int K, int NQ, int NSL, int ND, bool FAR>
+__device__ __forceinline__ void eval_cell_sp(const float4* __restrict__ srec, const int4* __restrict__ svid,
+                                             const dq* __restrict__ snrm, const float4* __restrict__ splane, int s0,
+                                             int s1, int nq, int4 tv, const float (&x)[K], const float (&y)[K],
+                                             const float (&z)[K], const float (&q2)[K], const float (&o)[3],
+                                             const double (&cen)[3], const double (&nrm)[3],
+                                             float (&sl)[NSL > 0 ? NSL : 1][K], float (&dl)[ND > 0 ? ND : 1][K])
+{
+  constexpr bool DL = ND > 0;
+  constexpr int NDX = ND > 0 ? ND : 1;
+  constexpr int NREC = rec_slots(NSL, ND);
+  constexpr int NS = NSL > 0 ? NSL : 1;
+  const int nqr = NQ > 0 ? NQ : nq;
+  float2 X[K], Y[K], Z[K], W[K], SL[NS][K], DLp[NDX][K];
+#pragma unroll
+  for (int a = 0; a < K; ++a) {
+    X[a] = make_float2(x[a], x[a]);
+    Y[a] = make_float2(y[a], y[a]);
+    Z[a] = make_float2(z[a], z[a]);
+    W[a] = make_float2(q2[a], q2[a]);
+#pragma unroll
+    for (int c = 0; c < NDX; ++c) DLp[c][a] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < NS; ++c) SL[c][a] = make_float2(0.f, 0.f);
+  }
+  const float2 half2 = make_float2(0.5f, 0.5f);
+  const float2 eps2 = make_float2(1e-24f, 1e-24f);
+#pragma unroll 1
+  for (int s = s0; s < s1; s += 2) {
+    float2 keep = make_float2(1.f, 1.f);
+    if constexpr (!FAR) {
+      const bool m0 = shares_vertex(tv, svid[s]), m1 = shares_vertex(tv, svid[s + 1]);
+      if (m0 && m1) continue;
+      keep = make_float2(m0 ? 0.f : 1.f, m1 ? 0.f : 1.f);
+    }
+    const float4* r = srec + (size_t)(s >> 1) * nqr * NREC * 2;
+    float2 acc2[NDX][K];
+#pragma unroll
+    for (int c = 0; c < NDX; ++c)
+#pragma unroll
+      for (int a = 0; a < K; ++a) acc2[c][a] = make_float2(0.f, 0.f);
+    // four DL columns hold 4 x K packed sums per pair: their loop stays rolled (no spills)
+#pragma unroll(NQ > 0 ? (kUnrollX2 > 0 ? kUnrollX2 : (ND >= 4 ? 1 : NQ)) : 1)
+    for (int b = 0; b < nqr; ++b) {
+      const float4* rv = r + b * NREC * 2;
+      const float2 px = sp_comp(rv, 0, 0), py = sp_comp(rv, 0, 1), pz = sp_comp(rv, 0, 2), pw = sp_comp(rv, 0, 3);
+      float2 ch[NS], sd[NDX];
+#pragma unroll
+      for (int c = 0; c < NSL; ++c) {
+        ch[c] = sp_comp(rv, charge_slot(c, ND), charge_comp(c, ND));
+        if constexpr (!FAR) ch[c] = __fmul2_rn(ch[c], keep);
+      }
+#pragma unroll
+      for (int c = 0; c < ND; ++c) {
+        sd[c] = sp_comp(rv, 1 + c / 4, c % 4);
+        if constexpr (!FAR) sd[c] = __fmul2_rn(sd[c], keep);
+      }
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        float2 r2;
+        if constexpr (FAR) {
+          r2 = __ffma2_rn(X[a], px, __ffma2_rn(Y[a], py, __ffma2_rn(Z[a], pz, __fadd2_rn(W[a], pw))));
+        } else {
+          const float2 dx = __ffma2_rn(half2, px, X[a]);
+          const float2 dy = __ffma2_rn(half2, py, Y[a]);
+          const float2 dz = __ffma2_rn(half2, pz, Z[a]);
+          r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+        }
+        const float2 inv = make_float2(rsq(r2.x), rsq(r2.y));
+#pragma unroll
+        for (int c = 0; c < NSL; ++c) SL[c][a] = __ffma2_rn(ch[c], inv, SL[c][a]);
+        if constexpr (ND == 1) {
+          acc2[0][a] = __ffma2_rn(__fmul2_rn(inv, inv), __fmul2_rn(sd[0], inv), acc2[0][a]);
+        } else if constexpr (ND > 1) {
+          const float2 inv3 = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+#pragma unroll
+          for (int c = 0; c < ND; ++c) acc2[c][a] = __ffma2_rn(sd[c], inv3, acc2[c][a]);
+        }
+      }
+    }
+    if constexpr (DL) {
+      // d = signed distance of each target point from the planes of triangles s, s+1
+      float2 nx, ny, nz, nw;
+      if constexpr (FAR) {
+        const float4 p0 = splane[s], p1 = splane[s + 1];
+        nx = make_float2(p0.x, p1.x); ny = make_float2(p0.y, p1.y); nz = make_float2(p0.z, p1.z);
+        nw = make_float2(-p0.w, -p1.w);
+      } else {
+        float pn[2][4];
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+          const dq nj = snrm[s + l];
+          const float dnx = (float)(nj.x - nrm[0]), dny = (float)(nj.y - nrm[1]), dnz = (float)(nj.z - nrm[2]);
+          pn[l][0] = dnx; pn[l][1] = dny; pn[l][2] = dnz;
+          pn[l][3] = (float)(cen[0] * nj.x + cen[1] * nj.y + cen[2] * nj.z - nj.w) + (o[0] * dnx + (o[1] * dny + o[2] * dnz));
+        }
+        nx = make_float2(pn[0][0], pn[1][0]); ny = make_float2(pn[0][1], pn[1][1]);
+        nz = make_float2(pn[0][2], pn[1][2]); nw = make_float2(pn[0][3], pn[1][3]);
+      }
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        const float2 d = __ffma2_rn(X[a], nx, __ffma2_rn(Y[a], ny, __ffma2_rn(Z[a], nz, nw)));
+#pragma unroll
+        for (int c = 0; c < ND; ++c) DLp[c][a] = __ffma2_rn(d, acc2[c][a], DLp[c][a]);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < K; ++a) {
+#pragma unroll
+    for (int c = 0; c < NSL; ++c) sl[c][a] += SL[c][a].x + SL[c][a].y;
+#pragma unroll
+    for (int c = 0; c < ND; ++c) dl[c][a] += DLp[c][a].x + DLp[c][a].y;
   }
 }
 

@@ -75,6 +75,42 @@ def test_large_mesh_sampled_rows_vs_oracle(gpu_lib, oracle, level, nrows):
         assert rel_l2(q32, q) < MIXED_TOL
 
 
+def test_odd_triangle_count_and_source_tiles(gpu_lib, oracle):
+    # The FP32 far kernel stages source triangles in pairs: an odd count (the
+    # last triangle paired with a zero-strength dummy) and odd requested tile
+    # sizes (rounded down to even, at least 2) must give the same operator.
+    nodes, elems = meshes.perturbed_icosphere(4, seed=3)
+    elems = elems[:-1]  # 5,119 triangles, an open surface
+    rng = np.random.default_rng(11)
+    t = rng.normal(size=elems.shape[0])
+    u = rng.normal(size=nodes.shape[0])
+    rows = np.unique(np.concatenate([[0, elems.shape[0] - 1],
+                                     rng.choice(elems.shape[0], 62, replace=False)])).astype(np.int32)
+    oracle.set_order(4)
+    vo, qo = oracle.apply_rows(nodes, elems, t, u, rows)
+    with gpu_lib.Mesh(nodes, elems) as m:
+        v, q = m.apply_sl_dl(t, u)
+        assert rel_l2(v[rows], vo) < FP64_TOL
+        assert rel_l2(q[rows], qo) < FP64_TOL
+        p1 = m.apply_sl_p1(u)
+        for tile in (0, 33, 7, 1):
+            m.set_plan(32, tile)
+            v32, q32 = m.apply_sl_dl(t, u, precision="mixed")
+            assert rel_l2(v32[rows], vo) < MIXED_TOL, tile
+            assert rel_l2(q32[rows], qo) < MIXED_TOL, tile
+            assert rel_l2(v32, v) < MIXED_TOL, tile
+            assert rel_l2(q32, q) < MIXED_TOL, tile
+            assert rel_l2(m.apply_sl(t, precision="mixed"), v) < MIXED_TOL, tile
+            assert rel_l2(m.apply_dl(u, precision="mixed"), q) < MIXED_TOL, tile
+            assert rel_l2(m.apply_sl_p1(u, precision="mixed"), p1) < MIXED_TOL, tile
+            # four DL columns per pass (near cells hold the target's own points)
+            G = rng.normal(size=(4, nodes.shape[0]))
+            b32, b64 = m.dirichlet_rhs(G, precision="mixed"), m.dirichlet_rhs(G)
+            assert np.isfinite(b32).all(), tile
+            for k in range(4):
+                assert rel_l2(b32[k], b64[k]) < MIXED_TOL, (tile, k)
+
+
 def test_applies_are_bitwise_reproducible(gpu_lib):
     nodes, elems = meshes.perturbed_icosphere(4, seed=2)
     rng = np.random.default_rng(0)
