@@ -664,7 +664,7 @@ def main():
                      "traffic": FAR_TRAFFIC_L6 if (args.level == LEVEL and args.far_engine == "cuda"
                                                    and plan_info.get("items_per_sm") == FAR_TRAFFIC_PLAN) else None,
                      "traffic_unit": "bytes per launch",
-                     "kernel": "far_tc_kernel" if args.far_engine == "tensor" else "far_kernel<float,7,7,1,true>",
+                     "kernel": "far_tc_kernel" if args.far_engine == "tensor" else "far_kernel<float,7,7,1,1,false>",
                      "far_ms": far_avg,
                      "per_pair": {"mufu_rsqrt": mufu_pp, "fma_pipe_ops": fma_pp, "tensor_flops": tc_pp},
                      "fma": {"achieved": fma_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
