@@ -9,40 +9,41 @@
 
 namespace eb {
 
-// Shape of the FP32 far kernel per variant. far_source_pairs: eval_cell_sp over
-// a source-pair tile, or eval_cell_x2 (target points in pairs) for the
-// variants with three or more SL charges unless EB_SP_WIDE, and for the
-// 8-point four-column DL variant, whose packed sums would spill.
-// far_min_blocks: resident CTAs per SM the registers are capped for; the
-// one-output variants (SL, P1-tested SL, DL up to 7 points) fit 3 without
-// spills, as do the wide SL variants in the target-pair form.
+// Shape of the FP32 far kernel per variant (measured at the L6 icosphere).
+// far_source_pairs: eval_cell_sp over a source-pair tile, or eval_cell_x2
+// (target points in pairs) for the variants with three or more SL charges
+// (3 and 4 right-hand sides: 90.5 / 100.7 ms against 94.6 / 103.4 ms in the
+// source-pair form) and for the 8-point four-column DL variant, whose packed
+// sums would spill. far_min_blocks: resident CTAs per SM the registers are
+// capped for: 3 for SL alone (77.7 against 82.1 ms) and the wide SL variants,
+// no spills in either; 2 for the rest (SL+DL and DL alone measured slower at 3).
 #ifndef EB_SP_WIDE
-#define EB_SP_WIDE 1
+#define EB_SP_WIDE 0
 #endif
-#ifndef EB_MINB_NARROW
-#define EB_MINB_NARROW EB_F32_MINB
+#ifndef EB_MINB_SL
+#define EB_MINB_SL 3
 #endif
 #ifndef EB_MINB_WIDE
-#define EB_MINB_WIDE EB_F32_MINB
+#define EB_MINB_WIDE 3
 #endif
 template <typename T, int K, int NSL, int ND>
 __host__ __device__ constexpr bool far_source_pairs()
 {
   return std::is_same<T, float>::value && kFarSourcePairs && !(K >= 8 && ND >= 4) && (NSL < 3 || EB_SP_WIDE);
 }
-template <typename T, int K, int NSL, int ND>
+template <typename T, int NSL, int ND, bool P1T>
 __host__ __device__ constexpr int far_min_blocks()
 {
-  return !std::is_same<T, float>::value     ? EB_F64_MINB
-         : NSL + ND == 1 && (NSL || K < 8) ? EB_MINB_NARROW
-         : NSL >= 3                         ? EB_MINB_WIDE
-                                            : EB_F32_MINB;
+  return !std::is_same<T, float>::value ? EB_F64_MINB
+         : NSL == 1 && ND == 0 && !P1T  ? EB_MINB_SL
+         : NSL >= 3                     ? EB_MINB_WIDE
+                                        : EB_F32_MINB;
 }
 
 // P1T: P1 test functions; the item's three outputs are sum_a w_a phi_k(x_a) acc_a
 // (k = 0, 1, 2 in the triangle's vertex order) of the single SL charge.
 template <typename T, int K, int NQ, int NSL, int ND, bool P1T>
-__global__ void __launch_bounds__(kTT, far_min_blocks<T, K, NSL, ND>())
+__global__ void __launch_bounds__(kTT, far_min_blocks<T, NSL, ND, P1T>())
     far_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
                int* __restrict__ counter)
 {
