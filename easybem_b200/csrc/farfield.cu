@@ -11,33 +11,32 @@ namespace eb {
 
 // Shape of the FP32 far kernel per variant (measured at the L6 icosphere).
 // far_source_pairs: eval_cell_sp over a source-pair tile, or eval_cell_x2
-// (target points in pairs) for the variants with three or more SL charges
-// (3 and 4 right-hand sides: 90.5 / 100.7 ms against 94.6 / 103.4 ms in the
-// source-pair form) and for the 8-point four-column DL variant, whose packed
-// sums would spill. far_min_blocks: resident CTAs per SM the registers are
-// capped for: 3 for SL alone (77.7 against 82.1 ms) and the wide SL variants,
-// no spills in either; 2 for the rest (SL+DL and DL alone measured slower at 3).
-#ifndef EB_SP_WIDE
-#define EB_SP_WIDE 0
+// (target points in pairs). The SL-only variants (1, 3 and 4 right-hand sides)
+// share one form, so that a column's sums are the same bits whichever variant
+// carries it (the batched solver and the server rely on that); they take
+// target pairs unless EB_SP_SL, because the 4-column variant, which the
+// batched solves and serving run, fits 3 CTAs per SM in that form (100.7 ms
+// against 103.4 ms for source pairs at 2 CTAs; 3 columns 90.5 against 94.6).
+// The 8-point four-column DL variant also keeps target pairs (its packed sums
+// would spill). far_min_blocks: resident CTAs per SM the registers are capped
+// for: 3 for the SL-only variants (no spills), 2 for SL+DL, DL and the
+// P1-tested SL (SL+DL at 3 spills: 113.5 against 108.4 ms; DL 101.2 against 99.3).
+#ifndef EB_SP_SL
+#define EB_SP_SL 0
 #endif
 #ifndef EB_MINB_SL
 #define EB_MINB_SL 3
 #endif
-#ifndef EB_MINB_WIDE
-#define EB_MINB_WIDE 3
-#endif
-template <typename T, int K, int NSL, int ND>
+template <typename T, int K, int NSL, int ND, bool P1T>
 __host__ __device__ constexpr bool far_source_pairs()
 {
-  return std::is_same<T, float>::value && kFarSourcePairs && !(K >= 8 && ND >= 4) && (NSL < 3 || EB_SP_WIDE);
+  return std::is_same<T, float>::value && kFarSourcePairs && !(K >= 8 && ND >= 4) &&
+         (ND > 0 || P1T || EB_SP_SL);
 }
 template <typename T, int NSL, int ND, bool P1T>
 __host__ __device__ constexpr int far_min_blocks()
 {
-  return !std::is_same<T, float>::value ? EB_F64_MINB
-         : NSL == 1 && ND == 0 && !P1T  ? EB_MINB_SL
-         : NSL >= 3                     ? EB_MINB_WIDE
-                                        : EB_F32_MINB;
+  return !std::is_same<T, float>::value ? EB_F64_MINB : ND == 0 && !P1T ? EB_MINB_SL : EB_F32_MINB;
 }
 
 // P1T: P1 test functions; the item's three outputs are sum_a w_a phi_k(x_a) acc_a
@@ -49,7 +48,7 @@ __global__ void __launch_bounds__(kTT, far_min_blocks<T, NSL, ND, P1T>())
 {
   using S = typename Slot<T>::type;
   constexpr bool F32 = std::is_same<T, float>::value;
-  constexpr bool SP = far_source_pairs<T, K, NSL, ND>();
+  constexpr bool SP = far_source_pairs<T, K, NSL, ND, P1T>();
   constexpr bool DL = ND > 0;
   constexpr int NDX = ND > 0 ? ND : 1;
   constexpr int NREC = rec_slots(NSL, ND);

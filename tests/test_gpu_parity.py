@@ -217,8 +217,11 @@ def test_batched_apply_equals_per_mesh_applies(gpu_lib):
                 for m, t, v in zip(ms, ts, d_v):
                     vv = v.cpu().numpy()
                     for c in range(ncols):
+                        # every SL-only variant evaluates a column with the same
+                        # arithmetic in the same order, whatever the column count
+                        # (the solver and the server rely on it), in both precisions
                         ref = m.apply_sl(t[c], precision=prec)
-                        assert rel_l2(vv[c], ref) <= (1e-14 if prec == "fp64" else 1e-7)
+                        assert rel_l2(vv[c], ref) <= (1e-14 if prec == "fp64" else 1e-12)
             bt.close()
     for m in ms:
         m.close()

@@ -52,7 +52,10 @@ def test_tensor_far_field_matches_oracle_and_cuda_cores(gpu_lib, golden_ops, ora
             # FP64 and the single operators keep the CUDA-core kernels
             v64, q64 = m.apply_sl_dl(t, u)
             assert rel_l2(v64[rows], vo) < 1e-12 and rel_l2(q64[rows], qo) < 1e-12
-            assert rel_l2(m.apply_sl(t, precision="mixed"), vc) < 1e-7
+            # (the SL-only kernel packs target points, the fused one source
+            # triangles: the same pairs summed in another order)
+            vs = m.apply_sl(t, precision="mixed")
+            assert rel_l2(vs[rows], vo) < MIXED_TOL and rel_l2(vs, vc) < MIXED_TOL
 
 
 def test_tensor_far_field_follows_plan_changes(gpu_lib):
