@@ -307,7 +307,7 @@ static int build_static(Mesh* m)
   std::vector<float4> pos32((size_t)ne * Q), tgt32((size_t)h.nitems * K), tgtw32((size_t)h.nitems * K);
   std::vector<dq> tgtw64((size_t)h.nitems * K);
   std::vector<dq> pos64((size_t)ne * Q), trin(ne), tgt64((size_t)h.nitems * K), tcent(h.nitems), tnrm(h.nitems),
-      ccent(h.ncells), snrm(ne), ttile(ntt), splane64(ne);
+      ccent(h.ncells), snrm(ne), ttile(ntt), twarp((h.nitems + kWarpItems - 1) / kWarpItems), splane64(ne);
   std::vector<float4> splane32(ne);
   std::vector<double> wjtab((size_t)ne * Q);
   std::vector<int4> svid(ne), tvid(h.nitems);
@@ -374,29 +374,35 @@ static int build_static(Mesh* m)
       }
     }
   }
-  // target-tile bounding spheres over the triangles of kTT consecutive items
-  for (int t = 0; t < ntt; t++) {
-    const int i0 = t * kTT, i1 = std::min(h.nitems, i0 + kTT);
-    d3 c = mk3(0, 0, 0);
-    for (int it = i0; it < i1; it++) c = c + mk3(tcent[it].x, tcent[it].y, tcent[it].z);
-    c = (1.0 / (i1 - i0)) * c;
-    double r2 = 0.0;
-    for (int it = i0; it < i1; it++)
-      for (int k = 0; k < 3; k++) {
-        const d3 v = vertex(it / h.nchunk, k);
-        r2 = std::max(r2, dot3(v - c, v - c));
-      }
-    ttile[t] = dq{c.x, c.y, c.z, std::sqrt(r2) * (1.0 + 1e-12)};
-  }
-  // how the tile x cell blocks split under the kernels' separation test
+  // bounding spheres over the triangles of n consecutive target items: per
+  // tile of kTT (the tensor-core kernel's test) and per warp of kWarpItems
+  // (the CUDA-core kernel's: a tighter sphere leaves fewer cells "near")
+  auto item_spheres = [&](int n, std::vector<dq>& out) {
+    for (size_t t = 0; t < out.size(); t++) {
+      const int i0 = (int)t * n, i1 = std::min(h.nitems, i0 + n);
+      d3 c = mk3(0, 0, 0);
+      for (int it = i0; it < i1; it++) c = c + mk3(tcent[it].x, tcent[it].y, tcent[it].z);
+      c = (1.0 / (i1 - i0)) * c;
+      double r2 = 0.0;
+      for (int it = i0; it < i1; it++)
+        for (int k = 0; k < 3; k++) {
+          const d3 v = vertex(it / h.nchunk, k);
+          r2 = std::max(r2, dot3(v - c, v - c));
+        }
+      out[t] = dq{c.x, c.y, c.z, std::sqrt(r2) * (1.0 + 1e-12)};
+    }
+  };
+  item_spheres(kTT, ttile);
+  item_spheres(kWarpItems, twarp);
+  // how the warp x cell blocks split under the CUDA-core kernel's separation test
   {
     long long fc = 0, nc = 0;
-    for (int t = 0; t < ntt; t++) {
-      const long long nt = std::min(h.nitems, (t + 1) * kTT) - t * kTT;  // target items of the tile
+    for (size_t t = 0; t < twarp.size(); t++) {
+      const long long nt = std::min<long long>(h.nitems, (long long)(t + 1) * kWarpItems) - (long long)t * kWarpItems;
       for (int c = 0; c < h.ncells; c++) {
         const long long ns = std::min(ne, (c + 1) * kCell) - c * kCell;
-        const double dx = ccent[c].x - ttile[t].x, dy = ccent[c].y - ttile[t].y, dz = ccent[c].z - ttile[t].z;
-        const double rr = kFarRatio * (ccent[c].w + ttile[t].w);
+        const double dx = ccent[c].x - twarp[t].x, dy = ccent[c].y - twarp[t].y, dz = ccent[c].z - twarp[t].z;
+        const double rr = kFarRatio * (ccent[c].w + twarp[t].w);
         (dx * dx + dy * dy + dz * dz > rr * rr ? fc : nc) += nt * ns;
       }
     }
@@ -419,6 +425,7 @@ static int build_static(Mesh* m)
                         part(m->tgt64, tgt64),   part(m->tgtw32, tgtw32),   part(m->tgtw64, tgtw64),
                         part(m->tcent, tcent),   part(m->tnrm, tnrm),       part(m->snrm, snrm),
                         part(m->tvid, tvid),     part(m->ccent, ccent),     part(m->ttile, ttile),
+                        part(m->twarp, twarp),
                         part(m->splane32, splane32), part(m->splane64, splane64)};
   auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
   size_t total = 0;
@@ -629,6 +636,7 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
   desc.svid = m->svid.as<int4>();
   desc.ccent = m->ccent.as<dq>();
   desc.ttile = m->ttile.as<dq>();
+  desc.twarp = m->twarp.as<dq>();
   desc.partial = partial;
   desc.nitems = h.nitems;
   desc.ne = h.ne;

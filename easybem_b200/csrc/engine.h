@@ -104,7 +104,7 @@ struct Mesh {
   // static geometry (sorted order), views into one allocation (arena)
   DevBuf arena;
   DevBuf pos32, pos64, wj, trin, svid, perm, iperm, bary;
-  DevBuf tgt32, tgt64, tgtw32, tgtw64, tcent, tnrm, tvid, ccent, snrm, ttile, splane32, splane64;
+  DevBuf tgt32, tgt64, tgtw32, tgtw64, tcent, tnrm, tvid, ccent, snrm, ttile, twarp, splane32, splane64;
   // P1 x P1 single layer near field (built on first use)
   DevBuf p1_rowptr, p1_col, p1_val;
   // near field

@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(kTT, far_min_blocks<T, NSL, ND, P1T>())
     const int ti = w.tgt0 + threadIdx.x;
     const bool active = ti < md.nitems;
     const int tsel = active ? ti : w.tgt0;
-    const dq tile = md.ttile[w.tgt0 / kTT];
+    // separation test per warp (the warp's items are consecutive in Morton order)
+    const dq tile = md.twarp[tsel / kWarpItems];
 
     // target points relative to the triangle centroid are re-read per cell
     // (L1-resident) rather than held in registers
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(kTT, far_min_blocks<T, NSL, ND, P1T>())
           const int cell = (t0 + g0) / kCell;
           const int g1 = min(ns, (cell + 1) * kCell - t0);
           const dq cc = md.ccent[cell];
-          // warp-uniform (tile-level) separation test
+          // warp-uniform separation test (the warp's bounding sphere against the cell's)
           const double ddx = cc.x - tile.x, ddy = cc.y - tile.y, ddz = cc.z - tile.z;
           const double rr = kFarRatio * (cc.w + tile.w);
           const bool far = ddx * ddx + ddy * ddy + ddz * ddz > rr * rr;

@@ -34,6 +34,7 @@ namespace eb {
 #define EB_TT 128
 #endif
 constexpr int kTT = EB_TT;  // target items (threads) per CTA
+constexpr int kWarpItems = 32;  // target items per warp: the CUDA-core kernel's separation test is per warp
 constexpr int kTS = 64;   // source triangles per shared-memory tile (Q <= 7)
 constexpr int kMaxRecSlots = 3;  // record slots of the widest variant
 constexpr int kMaxOutputs = 5;   // SL charges + DL of the widest variant
@@ -67,13 +68,15 @@ __host__ __device__ constexpr int rec_slots(int nsl, int nd) { return 1 + (nsl +
 __host__ __device__ constexpr int charge_slot(int r, int nd) { return 1 + (r + nd) / 4; }
 __host__ __device__ constexpr int charge_comp(int r, int nd) { return (r + nd) % 4; }
 
-// A source cell is "far" from a target tile when the distance of their
-// bounding-sphere centres exceeds kFarRatio times the sum of the radii (which
-// bound every vertex): no shared vertex is possible (any ratio above 1), and
-// |x|^2 + |y|^2 - 2 x.y loses at most ((k+1)/(k-1))^2 ulps to cancellation
-// for the closest pairs (k = kFarRatio; 19 at 1.6). Measured at the L6
-// icosphere: 1.6 leaves 9 % of the (target, source triangle) pairs in the
-// other cells (20 % at 2.5) with the same mixed-precision error (9e-8).
+// A source cell is "far" from a group of target items (a warp's 32 in the
+// CUDA-core kernel, a 128-item tile in the tensor-core kernel) when the
+// distance of their bounding-sphere centres exceeds kFarRatio times the sum
+// of the radii (which bound every vertex): no shared vertex is possible (any
+// ratio above 1), and |x|^2 + |y|^2 - 2 x.y loses at most ((k+1)/(k-1))^2
+// ulps to cancellation for the closest pairs (k = kFarRatio; 19 at 1.6).
+// Measured at the L6 icosphere with 128-item groups: 1.6 leaves 9 % of the
+// (target, source triangle) pairs in the other cells (20 % at 2.5) with the
+// same mixed-precision error (9e-8); per warp it leaves 4 %.
 #ifndef EB_FAR_RATIO
 #define EB_FAR_RATIO 1.6
 #endif
@@ -95,6 +98,7 @@ struct FarMeshDesc {
   const int4* svid;     // [ne]: vertex ids of sorted source triangles
   const dq* ccent;      // [ncells]: cell centre and bounding radius (FP64)
   const dq* ttile;      // [ntiles]: target-tile centre and bounding radius (FP64)
+  const dq* twarp;      // [nitems / kWarpItems, rounded up]: the same per warp of target items
   double* partial;      // [nout][nsplit][nitems]
   const int* active;    // optional: skip this mesh's work while *active == 0
   // tensor-core kernel only: source operands per cell (UMMA layout) and charges

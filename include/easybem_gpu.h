@@ -70,14 +70,14 @@ int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes);
  * the far-field partial sums that the same launch performs. No counterpart
  * in the reference. */
 int eb_mesh_near_field_bytes(eb_mesh mesh, long long* spmv_bytes, long long* fold_bytes);
-/* (target item, source triangle) pairs of the far-field work (each tile of
- * 128 target items x each 32-triangle source cell) in source cells well
- * separated from the tile (centre distance above 2.5 x the sum of the
- * bounding radii: expanded |x - y|^2, on the tensor cores when that engine
- * is on) and in the other cells (vertex mask and direct differences on the
- * CUDA cores). A target item is a triangle for rules of up to 7 points
- * (then the sum is nelems^2), a chunk of 8 of its points otherwise. No
- * counterpart in the reference. */
+/* (target item, source triangle) pairs of the far-field work (each warp of
+ * 32 target items x each 32-triangle source cell) in source cells well
+ * separated from the warp's items (centre distance above 1.6 x the sum of the
+ * bounding radii: no vertex mask, expanded |x - y|^2) and in the other cells
+ * (vertex mask and direct differences), as the CUDA-core far kernel splits
+ * them. A target item is a triangle for rules of up to 7 points (then the sum
+ * is nelems^2), a chunk of 8 of its points otherwise. No counterpart in the
+ * reference. */
 int eb_mesh_cell_pairs(eb_mesh mesh, long long* far_cell_tri_pairs, long long* near_cell_tri_pairs);
 
 /* v = V t, the P0 single layer (Galerkin, kernel 1/(4 pi |x-y|)); t and v
