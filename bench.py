@@ -51,9 +51,9 @@ FLOPS_PER_PAIR = 2 * FMA_OPS_PER_PAIR
 RSQRT_PER_PAIR = 1
 # DRAM bytes (read + write) of one CUDA-core far-field launch on the L6 workload under the
 # plan of 512 work items per SM (the autotuner's choice there), from an ncu capture of that
-# launch: 47.15 MB read (records, target tables) + 110.01 MB written (the partial sums of
+# launch: 46.94 MB read (records, target tables) + 107.84 MB written (the partial sums of
 # the 117-way source split).
-FAR_TRAFFIC_L6 = 47.15e6 + 110.01e6
+FAR_TRAFFIC_L6 = 46.94e6 + 107.84e6
 FAR_TRAFFIC_PLAN = 512
 
 
