@@ -163,6 +163,19 @@ class Mesh:
         check(lib().eb_apply_near_precond(self._h, _ptr(x), _ptr(y)))
         return y
 
+    @property
+    def topology_on_device(self) -> bool:
+        """True when the near-pair lists were built on the GPU (large meshes)."""
+        v = ctypes.c_int()
+        check(lib().eb_mesh_topology_on_device(self._h, ctypes.byref(v)))
+        return bool(v.value)
+
+    def near_field_bytes(self):
+        """(near-field SpMV bytes, far partial-sum fold bytes) of one fused apply."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().eb_mesh_near_field_bytes(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def cell_pairs(self):
         """(triangle pairs in well-separated source cells, in the other cells)."""
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
@@ -207,6 +220,18 @@ class Mesh:
         check(lib().eb_autotune(self._h, precision_code(precision), ops, int(reps), ctypes.byref(a), ctypes.byref(b),
                                 ctypes.byref(ms), ctypes.byref(ms0)))
         return {"items_per_sm": a.value, "src_tile": b.value, "ms": ms.value, "start_ms": ms0.value}
+
+
+def set_device_topology_min(nelems: int):
+    """Meshes created from now on with at least nelems triangles build their
+    near-pair lists on the GPU (default 65,536; 0: every mesh; 2**31 - 1: none)."""
+    check(lib().eb_set_device_topology_min(int(nelems)))
+
+
+def device_topology_min() -> int:
+    v = ctypes.c_int()
+    check(lib().eb_get_device_topology_min(ctypes.byref(v)))
+    return v.value
 
 
 def save_plans(path: str):

@@ -561,7 +561,16 @@ int mesh_create(int nv, const double* nodes, int ne, const int* elems1, int orde
   cudaGetDevice(&m->device);
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
-  int st = prepare_host_mesh(nv, nodes, ne, elems1, order, &m->h);
+  // large meshes build the near-pair lists on the GPU (host_topology otherwise,
+  // and when a row has too many candidates for the device pass)
+  const bool dev_topology = ne >= device_topology_min();
+  int st = prepare_host_mesh(nv, nodes, ne, elems1, order, &m->h, !dev_topology);
+  if (st == EB_OK && dev_topology) {
+    bool done = false;
+    st = device_topology(&m->h, &done);
+    if (st == EB_OK && !done) host_topology(&m->h);
+    m->h.topology_on_device = done;
+  }
   if (st == EB_OK) tuned_plan_for(m->h, &m->plan.items_per_sm, &m->plan.tile);
   const auto t1 = clk::now();
   if (st == EB_OK) st = build_static(m);
@@ -859,6 +868,13 @@ int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes)
   long long b = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8);
   b += 2 * 8LL * mesh->m->plan.nsplit * h.nitems + 2 * 8 * ne + 8 * ne /* trin */ + 4 * ne /* iperm */;
   *bytes = b;
+  return EB_OK;
+}
+
+int eb_mesh_topology_on_device(eb_mesh mesh, int* on_device)
+{
+  if (!mesh || !on_device) return set_error(EB_ERR_INVALID, "null argument");
+  *on_device = mesh->m->h.topology_on_device ? 1 : 0;
   return EB_OK;
 }
 

@@ -30,7 +30,8 @@ static uint64_t spread21(uint64_t x)
   return x;
 }
 
-int prepare_host_mesh(int nv, const double* nodes, int ne, const int* elems1, int order, HostMesh* m)
+int prepare_host_mesh(int nv, const double* nodes, int ne, const int* elems1, int order, HostMesh* m,
+                      bool topology)
 {
   if (nv < 3 || ne < 1 || !nodes || !elems1)
     return set_error(EB_ERR_INVALID, "mesh needs >= 3 vertices, >= 1 triangle and non-null arrays");
@@ -104,7 +105,13 @@ int prepare_host_mesh(int nv, const double* nodes, int ne, const int* elems1, in
   }
   target_split(m->Q, &m->K, &m->nchunk);
   m->nitems = ne * m->nchunk;
+  if (topology) host_topology(m);
+  return EB_OK;
+}
 
+void host_topology(HostMesh* m)
+{
+  const int nv = m->nv, ne = m->ne;
   // Vertex -> triangles.
   std::vector<int> vptr(nv + 1, 0), vtri(3 * (size_t)ne);
   for (int i = 0; i < 3 * ne; i++) vptr[m->elems[i] + 1]++;
@@ -124,8 +131,6 @@ int prepare_host_mesh(int nv, const double* nodes, int ne, const int* elems1, in
   m->dl_col.clear();
   std::vector<int> cand;
   std::vector<std::pair<int, int>> dl_entries;  // (column, entry id)
-  std::vector<int> slot_of_entry;               // built per row, flattened later
-  std::vector<std::vector<int>> contrib_rows;   // temporary per-slot lists
   long long near_incl_repeat = 0;
   std::vector<int> contrib_ptr(1, 0), contrib;
   for (int i = 0; i < ne; i++) {
@@ -166,7 +171,6 @@ int prepare_host_mesh(int nv, const double* nodes, int ne, const int* elems1, in
   m->dl_contrib_ptr.swap(contrib_ptr);
   m->dl_contrib.swap(contrib);
   m->far_quad_pairs = ((long long)ne * ne - near_incl_repeat) * (long long)m->Q * m->Q;
-  return EB_OK;
 }
 
 }  // namespace eb

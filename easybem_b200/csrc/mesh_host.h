@@ -43,15 +43,30 @@ struct HostMesh {
   std::vector<int> dl_contrib_ptr, dl_contrib;  // slot -> entries, ascending
 
   long long far_quad_pairs = 0;  // regular quadrature-point pairs per apply
+  bool topology_on_device = false;  // near-pair lists built by device_topology
   // (target item, source triangle) pairs in source cells well separated from
-  // the item's target tile, and in the others (where a far-field kernel
+  // the item's warp of target items, and in the others (where a far-field kernel
   // masks vertex-sharing pairs and forms differences directly); set with the
   // static tables
   long long far_cell_tri_pairs = 0, near_cell_tri_pairs = 0;
 };
 
-// Validates and prepares; returns EB_OK or an error status with a message.
-int prepare_host_mesh(int nv, const double* nodes, int ne, const int* elems1, int order, HostMesh* m);
+// Validates and prepares (Morton order, cells, target items and, when
+// topology is set, the near-pair CSR through host_topology); returns EB_OK or
+// an error status with a message.
+int prepare_host_mesh(int nv, const double* nodes, int ne, const int* elems1, int order, HostMesh* m,
+                      bool topology = true);
+
+// The near-pair CSR (sl_*, pair_*, dl_*) and far_quad_pairs of a prepared
+// mesh, on the host. device_topology (topology.cu) builds the same arrays on
+// the GPU for large meshes.
+void host_topology(HostMesh* m);
+
+// The same arrays built on the current GPU (topology.cu); *done is false when
+// a row has too many candidates and the caller must use host_topology.
+int device_topology(HostMesh* m, bool* done);
+// Meshes with at least this many triangles use device_topology.
+int device_topology_min();
 
 // Target items per triangle and points per item for Q quadrature points.
 void target_split(int Q, int* K, int* nchunk);

@@ -79,6 +79,17 @@ int eb_mesh_near_field_bytes(eb_mesh mesh, long long* spmv_bytes, long long* fol
  * is nelems^2), a chunk of 8 of its points otherwise. No counterpart in the
  * reference. */
 int eb_mesh_cell_pairs(eb_mesh mesh, long long* far_cell_tri_pairs, long long* near_cell_tri_pairs);
+/* Meshes with at least nelems triangles build their near-pair topology (the
+ * CSR lists of vertex-sharing triangle pairs and the double-layer vertex
+ * columns of the Sauter-Schwab near field) on the GPU; smaller meshes, and a
+ * mesh with a triangle that has more than 48 vertex-sharing neighbours
+ * (counted with repeats), build it on the host. Both give the same lists.
+ * Default 65,536; 0: every mesh; INT_MAX: none. The reference builds its
+ * topology on the host (src/meshTopology.cpp:22-261). */
+int eb_set_device_topology_min(int nelems);
+int eb_get_device_topology_min(int* nelems);
+/* 1 when the mesh's near-pair topology was built on the GPU, else 0. */
+int eb_mesh_topology_on_device(eb_mesh mesh, int* on_device);
 
 /* v = V t, the P0 single layer (Galerkin, kernel 1/(4 pi |x-y|)); t and v
  * have nelems entries, host memory. Replaces applyGPULaplace3d1Layer(t, v, 0)
