@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(128) topology_rows_kernel(
 
 namespace {
 
-std::atomic<int> g_device_topology_min{65536};
+std::atomic<int> g_device_topology_min{INT_MAX};
 
 // out[0..n) = exclusive prefix sums of in[0..n), on st.
 int exclusive_scan(const int* in, int* out, int n, cudaStream_t st)
@@ -246,7 +246,8 @@ int device_topology(HostMesh* h, bool* done)
   {
     TmpBuf d_elems(st), vcount(st), vptr(st), cursor(st), vtri(st), cnt(st), eptr(st), flags(st);
     EB_CHECK(d_elems.alloc(sizeof(int) * 3 * (size_t)ne));
-    EB_CHECK(copy_h2d(d_elems.p, h->elems.data(), sizeof(int) * 3 * (size_t)ne));
+    // stream-ordered like the scratch it fills (pageable source: staged by the driver)
+    EB_CUDA(cudaMemcpyAsync(d_elems.p, h->elems.data(), sizeof(int) * 3 * (size_t)ne, cudaMemcpyHostToDevice, st));
     EB_CHECK(vcount.alloc(sizeof(int) * nv));
     EB_CHECK(vptr.alloc(sizeof(int) * (nv + 1)));
     EB_CHECK(cursor.alloc(sizeof(int) * nv));
