@@ -92,33 +92,29 @@ __global__ void copy_total_kernel(const int* __restrict__ in, const int* __restr
 }
 
 // Lexicographic order of (column, entry) pairs.
-__device__ __forceinline__ bool less2(int2 a, int2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); }
+__host__ __device__ inline bool less2(int2 a, int2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); }
 
-// One test triangle per thread. FILL = false: counts of the row's pairs
-// (repeated triangles excluded), DL vertex columns and DL entries, and the
+// One test triangle's row. FILL = false: counts of the row's pairs (repeated
+// triangles excluded), DL vertex columns and DL entries, and in *nuniq the
 // candidates including repeats (for the far-field pair count). FILL = true:
 // the row written at the scanned offsets. Pairs are in ascending trial index
 // and DL entries in ascending (column, entry id) order, as on the host.
+// Returns false when the row has more than kMaxCand candidates.
 template <bool FILL>
-__global__ void __launch_bounds__(128) topology_rows_kernel(
-    const int* __restrict__ elems, const int* __restrict__ vptr, const int* __restrict__ vtri, int ne,
-    int* __restrict__ slcnt, int* __restrict__ dlcnt, int* __restrict__ ecnt,
-    unsigned long long* __restrict__ ncand, int* __restrict__ overflow, const int* __restrict__ slptr,
-    const int* __restrict__ dlptr, const int* __restrict__ eptr, int* __restrict__ sl_col, int* __restrict__ pair_i,
-    int8_t* __restrict__ pair_kind, int* __restrict__ dl_col, int* __restrict__ cptr, int* __restrict__ contrib)
+__host__ __device__ inline bool topology_row(int i, const int* __restrict__ elems, const int* __restrict__ vptr,
+                                             const int* __restrict__ vtri, int* nuniq, int* nsl_out, int* ndl_out,
+                                             int* nde_out, int p0, int g0, int e0, int* __restrict__ sl_col,
+                                             int* __restrict__ pair_i, int8_t* __restrict__ pair_kind,
+                                             int* __restrict__ dl_col, int* __restrict__ cptr,
+                                             int* __restrict__ contrib)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ne) return;
   const int fi[3] = {elems[3 * i], elems[3 * i + 1], elems[3 * i + 2]};
   int cand[kMaxCand];
   int nc = 0;
   for (int k = 0; k < 3; ++k) {
     const int v = fi[k];
     for (int p = vptr[v]; p < vptr[v + 1]; ++p) {
-      if (nc == kMaxCand) {
-        atomicExch(overflow, 1);
-        return;
-      }
+      if (nc == kMaxCand) return false;
       cand[nc++] = vtri[p];
     }
   }
@@ -135,11 +131,10 @@ __global__ void __launch_bounds__(128) topology_rows_kernel(
   int nu = 0;
   for (int a = 0; a < nc; ++a)
     if (a == 0 || cand[a] != cand[a - 1]) cand[nu++] = cand[a];
-  if (!FILL) atomicAdd(ncand, (unsigned long long)nu);
+  *nuniq = nu;
 
   int2 de[3 * kMaxCand];
   int nde = 0, nsl = 0;
-  const int p0 = FILL ? slptr[i] : 0;
   for (int u = 0; u < nu; ++u) {
     const int j = cand[u];
     const int fj[3] = {elems[3 * j], elems[3 * j + 1], elems[3 * j + 2]};
@@ -170,18 +165,46 @@ __global__ void __launch_bounds__(128) topology_rows_kernel(
     int ndl = 0;
     for (int e = 0; e < nde; ++e)
       if (e == 0 || de[e].x != de[e - 1].x) ++ndl;
-    slcnt[i] = nsl;
-    dlcnt[i] = ndl;
-    ecnt[i] = nde;
-    return;
+    *nsl_out = nsl;
+    *ndl_out = ndl;
+    *nde_out = nde;
+    return true;
   }
   // columns, their entries, and each column's end offset in the entry list
-  int gcol = dlptr[i] - 1;
-  const int e0 = eptr[i];
+  int gcol = g0 - 1;
   for (int e = 0; e < nde; ++e) {
     if (e == 0 || de[e].x != de[e - 1].x) dl_col[++gcol] = de[e].x;
     contrib[e0 + e] = de[e].y;
     if (e == nde - 1 || de[e + 1].x != de[e].x) cptr[gcol + 1] = e0 + e + 1;
+  }
+  return true;
+}
+
+// One test triangle per thread: topology_row, counting (FILL = false) or
+// writing at the scanned offsets (FILL = true).
+template <bool FILL>
+__global__ void __launch_bounds__(128) topology_rows_kernel(
+    const int* __restrict__ elems, const int* __restrict__ vptr, const int* __restrict__ vtri, int ne,
+    int* __restrict__ slcnt, int* __restrict__ dlcnt, int* __restrict__ ecnt,
+    unsigned long long* __restrict__ ncand, int* __restrict__ overflow, const int* __restrict__ slptr,
+    const int* __restrict__ dlptr, const int* __restrict__ eptr, int* __restrict__ sl_col, int* __restrict__ pair_i,
+    int8_t* __restrict__ pair_kind, int* __restrict__ dl_col, int* __restrict__ cptr, int* __restrict__ contrib)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  int nu = 0, nsl = 0, ndl = 0, nde = 0;
+  const bool ok = topology_row<FILL>(i, elems, vptr, vtri, &nu, &nsl, &ndl, &nde, FILL ? slptr[i] : 0,
+                                     FILL ? dlptr[i] : 0, FILL ? eptr[i] : 0, sl_col, pair_i, pair_kind, dl_col,
+                                     cptr, contrib);
+  if (!ok) {
+    atomicExch(overflow, 1);
+    return;
+  }
+  if (!FILL) {
+    atomicAdd(ncand, (unsigned long long)nu);
+    slcnt[i] = nsl;
+    dlcnt[i] = ndl;
+    ecnt[i] = nde;
   }
 }
 
