@@ -224,7 +224,7 @@ class Mesh:
 
 def set_device_topology_min(nelems: int):
     """Meshes created from now on with at least nelems triangles build their
-    near-pair lists on the GPU (default 2**31 - 1: none; 0: every mesh)."""
+    near-pair lists on the GPU (default 65,536; 0: every mesh; 2**31 - 1: none)."""
     check(lib().eb_set_device_topology_min(int(nelems)))
 
 

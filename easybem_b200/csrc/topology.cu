@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(128) topology_rows_kernel(
 
 namespace {
 
-std::atomic<int> g_device_topology_min{INT_MAX};
+std::atomic<int> g_device_topology_min{65536};
 
 // out[0..n) = exclusive prefix sums of in[0..n), on st.
 int exclusive_scan(const int* in, int* out, int n, cudaStream_t st)

@@ -84,7 +84,9 @@ int eb_mesh_cell_pairs(eb_mesh mesh, long long* far_cell_tri_pairs, long long* n
  * columns of the Sauter-Schwab near field) on the GPU; smaller meshes, and a
  * mesh with a triangle that has more than 48 vertex-sharing neighbours
  * (counted with repeats), build it on the host. Both give the same lists.
- * Default INT_MAX (none); 0: every mesh. The reference builds its
+ * Default 65,536; 0: every mesh; INT_MAX: none. Creating an L7 icosphere
+ * (327,680 triangles) took 732 ms with it against 904 ms on the host. The
+ * reference builds its
  * topology on the host (src/meshTopology.cpp:22-261). */
 int eb_set_device_topology_min(int nelems);
 int eb_get_device_topology_min(int* nelems);

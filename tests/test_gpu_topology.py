@@ -99,9 +99,11 @@ def test_device_topology_falls_back_for_high_valence(threshold):
         assert np.array_equal(a, b)
 
 
-def test_threshold_setting(gpu_lib):
-    assert gpu_lib.device_topology_min() == NEVER  # the default: host topology
+def test_default_threshold_puts_large_meshes_on_the_device(gpu_lib):
+    assert gpu_lib.device_topology_min() == 65536
     with gpu_lib.Mesh(*meshes.perturbed_icosphere(1, seed=0)) as m:
         assert not m.topology_on_device
+    with gpu_lib.Mesh(*meshes.perturbed_icosphere(6, seed=1)) as m:  # 81,920 triangles
+        assert m.topology_on_device and m.near_pairs == 1064900
     with pytest.raises(Exception):
         gpu_lib.set_device_topology_min(-1)
