@@ -55,6 +55,13 @@ RSQRT_PER_PAIR = 1
 # the 117-way source split).
 FAR_TRAFFIC_L6 = 46.94e6 + 107.84e6
 FAR_TRAFFIC_PLAN = 512
+# Far-field engines of the fused mixed apply and their kernels.
+ENGINES = ("cuda", "sym", "tensor")
+ENGINE_KERNELS = {"cuda": "far_kernel<float,7,7,1,1,false>", "sym": "far_sym_kernel",
+                  "tensor": "far_tc_kernel"}
+ENGINE_BOUNDS = {"cuda": "FMA pipe and MUFU together",
+                 "sym": "FMA pipe (one MUFU rsqrt per two ordered pairs)",
+                 "tensor": "MUFU reciprocal square root (tensor cores carry the distance GEMMs)"}
 
 
 def parse_args(argv=None):
@@ -75,9 +82,10 @@ def parse_args(argv=None):
     p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
     p.add_argument("--serve-sample", type=int, default=300,
                    help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
-    p.add_argument("--far-engine", default="cuda", choices=["tensor", "cuda"],
-                   help="matvec: far field of the mixed apply on the tensor cores (tcgen05 distance GEMMs) or on "
-                        "the FP32 pipes only; the other engine is timed beside it")
+    p.add_argument("--far-engine", default="cuda", choices=list(ENGINES),
+                   help="matvec: far field of the mixed apply on the FP32 pipes over every ordered pair (cuda), "
+                        "over every unordered pair once, added to both rows (sym), or with tcgen05 distance "
+                        "GEMMs (tensor); the other engines are timed beside it")
     p.add_argument("--no-extras", action="store_true",
                    help="matvec: skip the batch (256 ellipsoids), large (L7) and small (L3 solve) records "
                         "that a one-GPU run adds to its line")
@@ -291,7 +299,8 @@ def batch_record(local, solves=True):
         return a.elapsed_time(b) / k
 
     out = {}
-    for key, prec, engine in (("mixed", "mixed", "cuda"), ("mixed_tensor", "mixed", "tensor"), ("fp64", "fp64", "cuda")):
+    for key, prec, engine in (("mixed", "mixed", "cuda"), ("mixed_sym", "mixed", "sym"),
+                              ("mixed_tensor", "mixed", "tensor"), ("fp64", "fp64", "cuda")):
         for m in ms:
             m.set_far_engine(engine)
         bt = eb.Batch(ms, precision=prec, sl_dl=True)
@@ -317,7 +326,9 @@ def batch_record(local, solves=True):
     cat = lambda L, k: np.concatenate([x[k] for x in L])
     err = {"fp64_sl": rel(cat(ev, 0), cat(ev, 2)), "mixed_sl": rel(cat(ev, 1), cat(ev, 2)),
            "fp64_dl": rel(cat(eq, 0), cat(eq, 2)), "mixed_dl": rel(cat(eq, 1), cat(eq, 2)), "oracle_rows": 64,
-           "mixed_vs_fp64_full": mixed_vs_fp64}
+           "mixed_vs_fp64_full": mixed_vs_fp64,
+           "mixed_sym_vs_fp64_full": {"sl": rel(out["mixed_sym_vq"][0], out["fp64_vq"][0]),
+                                      "dl": rel(out["mixed_sym_vq"][1], out["fp64_vq"][1])}}
     # 4 SL right-hand sides per mesh (the Dirichlet data of the solves)
     rhs = [m.dirichlet_rhs(np.stack([1.0 / np.linalg.norm(it["nodes"] - p, axis=1) for p in it["sources"]]))
            for m, it in zip(ms, items)]
@@ -330,8 +341,10 @@ def batch_record(local, solves=True):
     rec = {"workload": "256 ellipsoids (icosphere L2-L5, 320-20,480 triangles), SL+DL batched apply "
                        "(one density pair per mesh), 4-RHS SL batched apply, GMRES(50)-IR to 1e-8",
            "quad_pairs_per_apply": int(pairs), "mesh_setup_s": t_create,
-           "sl_dl_mixed": out["mixed"], "sl_dl_mixed_tensor_cores": out["mixed_tensor"], "sl_dl_fp64": out["fp64"],
+           "sl_dl_mixed": out["mixed"], "sl_dl_mixed_symmetric": out["mixed_sym"],
+           "sl_dl_mixed_tensor_cores": out["mixed_tensor"], "sl_dl_fp64": out["fp64"],
            "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
+           "mixed_symmetric_over_fp64": out["mixed_sym"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "mixed_tensor_cores_over_fp64": out["mixed_tensor"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "rel_err_vs_oracle": err,
            "sl_4rhs_mixed": {"ms_per_apply": ms4, "Gpairs_per_s": pairs / (ms4 * 1e-3) / 1e9,
@@ -372,7 +385,7 @@ def large_record(local, solve=False):
     t_create = time.perf_counter() - t0
     m.set_profiling(True)
     res = {}
-    for prec, engine in (("mixed_cuda", "cuda"), ("fp64", "cuda"), ("mixed", "tensor")):
+    for prec, engine in (("mixed_cuda", "cuda"), ("fp64", "cuda"), ("mixed", "tensor"), ("mixed_sym", "sym")):
         m.set_far_engine(engine)
         p = "fp64" if prec == "fp64" else "mixed"
         m.apply_sl_dl(t, u, precision=p)
@@ -402,6 +415,10 @@ def large_record(local, solve=False):
                                   "frac_of_pair_bound": rate_t / bound_t,
                                   "rel_err_sl": rel(res["mixed"][0][rows], vo),
                                   "rel_err_dl": rel(res["mixed"][1][rows], qo)},
+           "mixed_symmetric": {"far_ms": res["mixed_sym"][2], "finalize_ms": res["mixed_sym"][3],
+                               "Gpairs_per_s": pairs / (res["mixed_sym"][2] * 1e-3) / 1e9,
+                               "rel_err_sl": rel(res["mixed_sym"][0][rows], vo),
+                               "rel_err_dl": rel(res["mixed_sym"][1][rows], qo)},
            "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
                     "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
            "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed_cuda"][0][rows], vo),
@@ -409,6 +426,7 @@ def large_record(local, solve=False):
                                  "fp64_sl": rel(res["fp64"][0][rows], vo), "fp64_dl": rel(res["fp64"][1][rows], qo),
                                  "oracle_rows": len(rows)}}
     rec["mixed_over_fp64"] = rec["mixed"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
+    rec["mixed_symmetric_over_fp64"] = rec["mixed_symmetric"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
     if solve:
         g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
         b = m.dirichlet_rhs(g)
@@ -553,12 +571,14 @@ def main():
     ms_fp64, far_fp64 = timed("fp64", k64, 1)
     v_64 = d_v.cpu().numpy()
     q_64 = d_q.cpu().numpy()
-    # the other far-field engine of the mixed apply, same plan
-    other = "cuda" if args.far_engine == "tensor" else "tensor"
-    mesh.set_far_engine(other)
-    ms_other, far_other = timed("mixed", max(2, args.steps // 3), 1)
-    v_other = d_v.cpu().numpy()
-    q_other = d_q.cpu().numpy()
+    # the other far-field engines of the mixed apply, same plan
+    others = {}
+    for other in ENGINES:
+        if other == args.far_engine:
+            continue
+        mesh.set_far_engine(other)
+        ms_o, far_o = timed("mixed", max(2, args.steps // 3), 1)
+        others[other] = (ms_o, far_o, d_v.cpu().numpy(), d_q.cpu().numpy())
     mesh.set_far_engine(args.far_engine)
 
     step_ms = max_over_ranks(sum(ms_mixed) / len(ms_mixed), dist, dev)
@@ -607,9 +627,8 @@ def main():
     # roofline of the dominant kernel (far field), event-timed on its stream
     far_avg = sum(f for f, _ in far_mixed) / len(far_mixed)
     fin_avg = sum(g for _, g in far_mixed) / len(far_mixed)
-    far_other_avg = sum(f for f, _ in far_other) / len(far_other)
     peak_tflops, peak_rsqrt = _measure_peak()
-    costs = {e: _engine_costs(e) for e in ("tensor", "cuda")}
+    costs = {e: _engine_costs(e) for e in ENGINES}
     mufu_pp, fma_pp, tc_pp = costs[args.far_engine]
     pair_rate = pairs / (far_avg * 1e-3)
     # pipe rates at this pair rate, and the pair rate the measured pipe peaks allow
@@ -648,23 +667,26 @@ def main():
                  "far_ms": sum(f for f, _ in far_fp64) / len(far_fp64)},
         "mixed_over_fp64": value / value64,
         "far_engine": args.far_engine,
-        "other_engine": {"engine": other, "ms_per_step": sum(ms_other) / len(ms_other), "far_ms": far_other_avg,
-                         "Gpairs_per_s": pairs / (far_other_avg * 1e-3) / 1e9,
-                         "rel_err_vs_oracle": {"sl": rel(v_other[rows], vo), "dl": rel(q_other[rows], qo)},
-                         "note": "the mixed apply with the other far-field engine, same plan and inputs"},
+        "other_engines": {e: {"ms_per_step": sum(o[0]) / len(o[0]),
+                              "far_ms": sum(f for f, _ in o[1]) / len(o[1]),
+                              "Gpairs_per_s": pairs / (sum(f for f, _ in o[1]) / len(o[1]) * 1e-3) / 1e9,
+                              "mixed_over_fp64": (pairs / (sum(o[0]) / len(o[0]) * 1e-3) / 1e9) / value64
+                              if value64 else None,
+                              "rel_err_vs_oracle": {"sl": rel(o[2][rows], vo), "dl": rel(o[3][rows], qo)},
+                              "kernel": ENGINE_KERNELS[e]}
+                          for e, o in others.items()},
         "near_cell_share": cell_near / (cell_far + cell_near),
         "rel_err_vs_oracle": err,
         "e2e": {"value": e2e_value, "unit": "Gpairs/s", "h2d_bytes_per_step": 8 * (ne + nv),
                 "d2h_bytes_per_step": 16 * ne, "ms_per_step": 1e3 * e2e_s},
         "gpu_launches": (4 if args.far_engine == "tensor" else 3) * args.steps,
-        "roofline": {"bound": ("MUFU reciprocal square root (tensor cores carry the distance GEMMs)"
-                               if args.far_engine == "tensor" else "FMA pipe and MUFU together"),
+        "roofline": {"bound": ENGINE_BOUNDS[args.far_engine],
                      "achieved": pair_rate / 1e9, "peak": pair_bound / 1e9, "unit": "Gpairs/s",
                      "frac": pair_rate / pair_bound,
                      "traffic": FAR_TRAFFIC_L6 if (args.level == LEVEL and args.far_engine == "cuda"
                                                    and plan_info.get("items_per_sm") == FAR_TRAFFIC_PLAN) else None,
                      "traffic_unit": "bytes per launch",
-                     "kernel": "far_tc_kernel" if args.far_engine == "tensor" else "far_kernel<float,7,7,1,1,false>",
+                     "kernel": ENGINE_KERNELS[args.far_engine],
                      "far_ms": far_avg,
                      "per_pair": {"mufu_rsqrt": mufu_pp, "fma_pipe_ops": fma_pp, "tensor_flops": tc_pp},
                      "fma": {"achieved": fma_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
@@ -724,7 +746,7 @@ def _engine_costs(engine):
     import ctypes
     from easybem_b200 import _lib
     a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-    _lib.check(_lib.lib().eb_far_engine_costs({"cuda": 0, "tensor": 1}[engine], ctypes.byref(a), ctypes.byref(b),
+    _lib.check(_lib.lib().eb_far_engine_costs({"cuda": 0, "tensor": 1, "sym": 2}[engine], ctypes.byref(a), ctypes.byref(b),
                                               ctypes.byref(c)))
     return a.value, b.value, c.value
 

@@ -26,6 +26,10 @@ __all__ = ["Mesh", "Batch", "Solver", "Server", "solve", "EasyBemError", "init_g
            "apply_gpu_laplace3d_hypersing", "version", "precision_code", "save_plans", "load_plans", "clear_plans"]
 
 
+# far-field engines of the fused mixed SL+DL apply (EB_FAR_* in easybem_gpu.h)
+FAR_ENGINES = {"cuda": 0, "tensor": 1, "sym": 2}
+
+
 def precision_code(precision) -> int:
     if precision in (None, "fp64", "double", EB_PREC_FP64):
         return EB_PREC_FP64
@@ -184,13 +188,15 @@ class Mesh:
 
     def set_far_engine(self, engine: str = "tensor"):
         """Far-field engine of the fused mixed SL+DL apply: "tensor" (tcgen05
-        GEMMs for the pair distances) or "cuda" (FP32 pipes only)."""
-        check(lib().eb_mesh_set_far_engine(self._h, {"cuda": 0, "tensor": 1}[engine]))
+        GEMMs for the pair distances), "cuda" (FP32 pipes only, every ordered
+        pair) or "sym" (FP32 pipes, every unordered pair once, added to both
+        rows)."""
+        check(lib().eb_mesh_set_far_engine(self._h, FAR_ENGINES[engine]))
 
     def far_engine(self, precision="mixed"):
         e = ctypes.c_int()
         check(lib().eb_mesh_get_far_engine(self._h, precision_code(precision), ctypes.byref(e)))
-        return "tensor" if e.value == 1 else "cuda"
+        return {v: k for k, v in FAR_ENGINES.items()}[e.value]
 
     def set_profiling(self, on: bool = True):
         check(lib().eb_set_profiling(self._h, 1 if on else 0))

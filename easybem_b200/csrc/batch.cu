@@ -1,4 +1,5 @@
 #include "batch.h"
+#include "farfield_sym.h"
 #include "farfield_tc.h"
 
 #include <algorithm>
@@ -55,6 +56,8 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   const int n = (int)entries.size();
   tc_ = fp32 && nsl_ == 1 && nd_ == 1;
   for (BatchEntry* be : entries) tc_ = tc_ && tc_eligible(be->mesh, fp32, 1, 1);
+  sym_ = fp32 && nsl_ == 1 && nd_ == 1 && !tc_;
+  for (BatchEntry* be : entries) sym_ = sym_ && sym_eligible(be->mesh, fp32, 1, 1);
   std::vector<TcPrepArgs> targs;
   std::vector<int> toff(1, 0);
   std::vector<FarMeshDesc> desc(n);
@@ -84,15 +87,33 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
                                  be->tc_be.as<float4>(), be->tc_charge.as<float>(), desc[e].active});
       toff.push_back(toff.back() + far_tc_prep_blocks(h.ncells));
     }
+    std::vector<WorkItem> sym_items;
+    int sym_nsplit = 0;
+    if (sym_) {  // the mesh's symmetric work list and its own zeroed partial slots
+      sym_nsplit = far_sym_items(h.nitems, h.ncells, kSymCellsPerItem, sym_items);
+      const size_t bytes = sizeof(double) * 2 * (size_t)sym_nsplit * h.nitems;
+      if (be->sym_partial.bytes < bytes) {
+        be->sym_partial.release();
+        EB_CHECK(be->sym_partial.alloc(bytes));
+        EB_CHECK(memset_sync(be->sym_partial.p, 0, bytes));
+      }
+      desc[e].partial = be->sym_partial.as<double>();
+      desc[e].nsplit = sym_nsplit;
+      desc[e].src_tile = kTS;
+    }
     src_tile = std::min(src_tile, desc[e].src_tile);
     args[e] = mesh_apply_args(m, fp32, be->rec.p, be->partial.as<double>(), nsl_ ? be->tin.as<double>() : nullptr,
                               h.ne, nd_ ? be->uin.as<double>() : nullptr, nsl_ ? be->vout.as<double>() : nullptr,
                               h.ne, nd_ ? be->qout.as<double>() : nullptr);
     args[e].active = d_flags ? d_flags + e : nullptr;
+    if (sym_) {
+      args[e].partial = be->sym_partial.as<double>();
+      args[e].nsplit = sym_nsplit;
+    }
     poff[e + 1] = poff[e] + (int)(((long long)h.ne * h.Q + kPrepBlock - 1) / kPrepBlock);
     foff[e + 1] = foff[e] + (h.ne + kFinalizeRows - 1) / kFinalizeRows;
     quad_pairs_ += h.far_quad_pairs;
-    for (WorkItem w : m->items_host) {
+    for (WorkItem w : sym_ ? sym_items : m->items_host) {
       w.mesh = e;
       const long long tg = std::min(kTT, h.nitems - w.tgt0);
       const long long src = (long long)std::min(h.ne, w.cell1 * kCell) - (long long)w.cell0 * kCell;
@@ -145,6 +166,10 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     grid_ = std::min(nsm, std::max(1, nitems_));
     occ_ = 1;
   }
+  if (sym_) {
+    occ_ = std::max(1, far_sym_occupancy());
+    grid_ = std::min(nsm * occ_, std::max(1, nitems_));
+  }
   return EB_OK;
 }
 
@@ -170,6 +195,8 @@ int Batch::run(cudaStream_t st, int reserve_sms)
   if (tc_)
     EB_CUDA(far_tc_launch(desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(),
                           tc_err_.as<int>(), grid, st));
+  else if (sym_)
+    EB_CUDA(far_sym_launch(desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(), grid, st));
   else
     EB_CUDA(far_launch(fp32_, nsl_, nd_, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
                        counter_.as<int>(), smem_, grid, st));

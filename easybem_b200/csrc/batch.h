@@ -28,6 +28,7 @@ struct BatchEntry {
   DevBuf tin, vout;     // kBatchCols columns of nelems each (inputs / outputs)
   DevBuf uin, qout;     // DL density [nnodes] and DL output [nelems] (batches with a DL column)
   DevBuf tc_be, tc_charge;  // tensor-core DL operand and charges (tensor-core SL+DL batches)
+  DevBuf sym_partial;       // symmetric SL+DL batches: partial slots (one per tile and row, zeroed once)
   int index = -1;       // position in the current batch
 };
 
@@ -52,6 +53,7 @@ class Batch {
 
   int nentries() const { return (int)entries_.size(); }
   bool tensor_cores() const { return tc_; }
+  bool symmetric() const { return sym_; }
   // EB_ERR_TIMEOUT (flag cleared) if the last tensor-core launch gave up a
   // bounded wait; the batch's stream must be synchronised.
   int check_error();
@@ -65,6 +67,7 @@ class Batch {
   DevBuf desc_, items_, args_, prep_off_, fin_off_, counter_;
   bool tc_ = false;  // far field on the tensor cores (fused FP32 SL+DL, 7-point rule, engine 1 on every mesh)
   DevBuf tc_args_, tc_off_, tc_err_;
+  bool sym_ = false;  // symmetric far field (fused FP32 SL+DL, 7-point rule, engine 2 on every mesh)
   int tc_blocks_ = 0;
   int nitems_ = 0, grid_ = 0, occ_ = 1, nsm_ = 148, prep_blocks_ = 0, fin_blocks_ = 0, K_ = 0, Q_ = 0;
   size_t smem_ = 0;

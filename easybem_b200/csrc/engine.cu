@@ -1,6 +1,7 @@
 // Device-resident mesh, FP64 Sauter-Schwab near field and the apply pipeline
 // (prep -> far field -> finalize), plus the C ABI of include/easybem_gpu.h.
 #include "engine.h"
+#include "farfield_sym.h"
 #include "farfield_tc.h"
 
 #include <algorithm>
@@ -546,6 +547,8 @@ int mesh_set_plan(Mesh* m, int items_per_sm, int tile)
   }
   m->tc_var.desc.release();
   m->tc_var.grid = 0;
+  m->sym_var.desc.release();
+  m->sym_var.grid = 0;
   m->rec.release();
   m->partial.release();
   return build_items(m);
@@ -659,6 +662,58 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
   return desc;
 }
 
+bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd)
+{
+  return m->plan.engine == 2 && fp32 && nsl == 1 && nd == 1 && m->h.Q == kSymRule && m->h.K == kSymRule &&
+         m->h.nchunk == 1;
+}
+
+int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd)
+{
+  if (sym_eligible(m, fp32, nsl, nd)) {
+    if (m->sym_nsplit > 0) return m->sym_nsplit;
+    std::vector<WorkItem> items;
+    return far_sym_items(m->h.nitems, m->h.ncells, kSymCellsPerItem, items);
+  }
+  return m->plan.nsplit;
+}
+
+// The symmetric far field: work list and zeroed partial slots once per mesh,
+// the descriptor once per scratch allocation, then the persistent kernel.
+static int sym_far_apply(Mesh* m, cudaStream_t st)
+{
+  const HostMesh& h = m->h;
+  if (!m->sym_partial.p) {
+    m->sym_nsplit = far_sym_items(h.nitems, h.ncells, kSymCellsPerItem, m->sym_items_host);
+    m->sym_nitems = (int)m->sym_items_host.size();
+    EB_CHECK(upload(m->sym_items, m->sym_items_host));
+    const size_t bytes = sizeof(double) * 2 * (size_t)m->sym_nsplit * h.nitems;
+    EB_CHECK(m->sym_partial.alloc(bytes));
+    EB_CUDA(cudaMemsetAsync(m->sym_partial.p, 0, bytes, st));
+  }
+  if (!m->sym_var.desc.p) {
+    FarMeshDesc desc = mesh_far_desc(m, true, 1, 1, m->rec.p, m->sym_partial.as<double>());
+    desc.nsplit = m->sym_nsplit;
+    desc.src_tile = kTS;
+    EB_CHECK(m->sym_var.desc.alloc(sizeof(FarMeshDesc)));
+    EB_CHECK(copy_h2d(m->sym_var.desc.p, &desc, sizeof desc));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    const int occ = std::max(1, far_sym_occupancy());
+    m->sym_var.grid = std::min(nsm * occ, std::max(1, m->sym_nitems));
+    m->sym_var.smem = far_sym_smem_bytes();
+    m->sym_var.src_tile = kTS;
+  }
+  EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
+  if (m->profile) EB_CUDA(cudaEventRecord(m->ev0, st));
+  EB_CUDA(far_sym_launch(m->sym_var.desc.as<FarMeshDesc>(), m->sym_items.as<WorkItem>(), m->sym_nitems,
+                         m->counter.as<int>(), m->sym_var.grid, st));
+  m->plan.grid = m->sym_var.grid;
+  m->tc_used = false;
+  m->sym_used = true;
+  return EB_OK;
+}
+
 bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd)
 {
   return m->plan.engine == 1 && fp32 && nsl == 1 && nd == 1 && m->h.Q == kTcRule && m->h.K == kTcRule;
@@ -754,16 +809,23 @@ int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const
     var.smem = smem;
     var.src_tile = desc.src_tile;
   }
-  const ApplyArgs A = mesh_apply_args(m, fp32, m->rec.p, m->partial.as<double>(), d_t, h.ne, d_u, d_v, h.ne, d_q);
+  const bool sym = sym_eligible(m, fp32, nsl, nd);
+  ApplyArgs A = mesh_apply_args(m, fp32, m->rec.p, m->partial.as<double>(), d_t, h.ne, d_u, d_v, h.ne, d_q);
   EB_CUDA(prep_launch(fp32, nsl, nd, A, st));
   if (m->profile && !m->ev0) {
     EB_CUDA(cudaEventCreate(&m->ev0));
     EB_CUDA(cudaEventCreate(&m->ev1));
     EB_CUDA(cudaEventCreate(&m->ev2));
   }
-  if (tc_eligible(m, fp32, nsl, nd)) {
+  if (sym) {
+    EB_CHECK(sym_far_apply(m, st));
+    A.partial = m->sym_partial.as<double>();
+    A.nsplit = m->sym_nsplit;
+  } else if (tc_eligible(m, fp32, nsl, nd)) {
+    m->sym_used = false;
     EB_CHECK(tc_far_apply(m, st));
   } else {
+    m->sym_used = false;
     EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
     if (m->profile) EB_CUDA(cudaEventRecord(m->ev0, st));
     EB_CUDA(far_launch(fp32, nsl, nd, h.K, h.Q, var.desc.as<FarMeshDesc>(), m->items.as<WorkItem>(), m->nitems_work,
@@ -771,8 +833,8 @@ int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const
     m->plan.grid = var.grid;
     m->tc_used = false;
   }
-  m->plan.smem = var.smem;
-  m->plan.src_tile = var.src_tile;
+  m->plan.smem = sym ? m->sym_var.smem : var.smem;
+  m->plan.src_tile = sym ? kTS : var.src_tile;
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev1, st));
   EB_CUDA(finalize_launch(nsl, nd, A, st));
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev2, st));
@@ -866,7 +928,8 @@ int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes)
   // per row: CSR row pointers, per entry column + value + gathered density,
   // the far-field partial sums of both outputs, the two outputs
   long long b = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8);
-  b += 2 * 8LL * mesh->m->plan.nsplit * h.nitems + 2 * 8 * ne + 8 * ne /* trin */ + 4 * ne /* iperm */;
+  b += 2 * 8LL * eb::mesh_far_nsplit(mesh->m, true, 1, 1) * h.nitems + 2 * 8 * ne + 8 * ne /* trin */ +
+       4 * ne /* iperm */;
   *bytes = b;
   return EB_OK;
 }
@@ -896,7 +959,7 @@ int eb_mesh_near_field_bytes(eb_mesh mesh, long long* spmv_bytes, long long* fol
   if (spmv_bytes) *spmv_bytes = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8) + 2 * 8 * ne;
   // the fold of the far-field partial sums: both outputs' partial slots, the
   // row's normal/area record and its permutation entry
-  if (fold_bytes) *fold_bytes = 2 * 8LL * mesh->m->plan.nsplit * h.nitems + 8 * ne + 4 * ne;
+  if (fold_bytes) *fold_bytes = 2 * 8LL * eb::mesh_far_nsplit(mesh->m, true, 1, 1) * h.nitems + 8 * ne + 4 * ne;
   return EB_OK;
 }
 
@@ -1053,8 +1116,8 @@ int eb_evaluate_potential(eb_mesh mesh, int precision, int npts, const double* p
 int eb_mesh_set_far_engine(eb_mesh mesh, int engine)
 {
   if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
-  if (engine != EB_FAR_CUDA_CORES && engine != EB_FAR_TENSOR_CORES)
-    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES or EB_FAR_TENSOR_CORES");
+  if (engine != EB_FAR_CUDA_CORES && engine != EB_FAR_TENSOR_CORES && engine != EB_FAR_SYMMETRIC)
+    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES, EB_FAR_TENSOR_CORES or EB_FAR_SYMMETRIC");
   mesh->m->plan.engine = engine;
   return EB_OK;
 }
@@ -1062,7 +1125,10 @@ int eb_mesh_set_far_engine(eb_mesh mesh, int engine)
 int eb_mesh_get_far_engine(eb_mesh mesh, int precision, int* engine)
 {
   if (!mesh || !engine) return set_error(EB_ERR_INVALID, "null argument");
-  *engine = eb::tc_eligible(mesh->m, precision == EB_PREC_MIXED, 1, 1) ? EB_FAR_TENSOR_CORES : EB_FAR_CUDA_CORES;
+  const bool fp32 = precision == EB_PREC_MIXED;
+  *engine = eb::tc_eligible(mesh->m, fp32, 1, 1)    ? EB_FAR_TENSOR_CORES
+            : eb::sym_eligible(mesh->m, fp32, 1, 1) ? EB_FAR_SYMMETRIC
+                                                    : EB_FAR_CUDA_CORES;
   return EB_OK;
 }
 
@@ -1074,8 +1140,14 @@ int eb_far_engine_costs(int engine, double* mufu_per_pair, double* fma_ops_per_p
     if (mufu_per_pair) *mufu_per_pair = 1.0;
     if (fma_ops_per_pair) *fma_ops_per_pair = 8.0;  // |x-y|^2 1 add + 3 FMA, SL 1 FMA, DL 2 mul + 1 FMA
     if (tensor_flops_per_pair) *tensor_flops_per_pair = 0.0;
+  } else if (engine == EB_FAR_SYMMETRIC) {
+    // one evaluation per unordered pair, i.e. per two ordered pairs: 1 MUFU,
+    // |x-y|^2 1 add + 3 FMA, r^3 2 mul, 4 FMA for the SL and DL sums of both orders
+    if (mufu_per_pair) *mufu_per_pair = 0.5;
+    if (fma_ops_per_pair) *fma_ops_per_pair = 5.0;
+    if (tensor_flops_per_pair) *tensor_flops_per_pair = 0.0;
   } else {
-    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES or EB_FAR_TENSOR_CORES");
+    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES, EB_FAR_TENSOR_CORES or EB_FAR_SYMMETRIC");
   }
   return EB_OK;
 }

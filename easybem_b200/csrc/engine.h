@@ -88,7 +88,7 @@ struct DevBuf {
 
 // Launch plan of the far field for one mesh (tile shape and work split).
 struct FarPlan {
-  int engine = 0;         // 0: CUDA-core far kernel; 1: tensor-core kernel where the variant has one
+  int engine = 0;         // 0: CUDA-core far kernel; 1: tensor-core kernel, 2: symmetric kernel, where the variant has one
   int items_per_sm = 32;  // work items per SM the source ranges are cut into (load balance)
   int tile = 0;           // source triangles per shared-memory tile (0: the variant's default)
   int src_tile = kTS;     // tile of the last launch
@@ -137,6 +137,14 @@ struct Mesh {
   Variant tc_var;
   bool tc_static_ready = false;
   bool tc_used = false;  // the last apply ran the tensor-core kernel
+  // symmetric far field (fused FP32 SL+DL, 7-point rule): its own work list
+  // and partial slots (one per target tile and row, zeroed once: slots no
+  // item writes stay zero), descriptor and launch shape
+  DevBuf sym_items, sym_partial;
+  std::vector<WorkItem> sym_items_host;
+  int sym_nitems = 0, sym_nsplit = 0;
+  Variant sym_var;
+  bool sym_used = false;  // the last apply ran the symmetric kernel
   // host seconds of mesh creation: topology and pairs, static tables, near
   // field, and within the tables their device allocation and copy
   double setup_s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -159,6 +167,12 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
 // True when mesh m applies the fused FP32 SL+DL far field with the
 // tensor-core kernel (engine 1, 7-point rule).
 bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd);
+// True when mesh m applies the fused FP32 SL+DL far field with the symmetric
+// kernel (engine 2, 7-point rule, one target item per triangle).
+bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd);
+// Partial slots per row of the far field the next apply in `precision` with
+// nsl SL and nd DL columns would fold.
+int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd);
 // The tensor-core distance operand of m (built once, synchronously).
 int ensure_tc_static(Mesh* m);
 // EB_ERR_TIMEOUT (and the flag cleared) if the last tensor-core launch on m

@@ -344,11 +344,18 @@ int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit
  * EB_FAR_TENSOR_CORES computes |x - y|^2 and the double-layer numerator
  * s (x - y).n of well-separated cells as split-TF32 GEMMs on the tensor
  * cores (tcgen05) and keeps the reciprocal square root and the sums on the
- * CUDA cores. Other variants always use the CUDA cores; get reports the
- * engine an apply in `precision` with both operators would use. No counterpart
- * in the reference. */
+ * CUDA cores; EB_FAR_SYMMETRIC evaluates every unordered quadrature-point
+ * pair once on the FP32 pipes and adds it to both rows of its triangle pair
+ * (the test and trial rules are the same rule, so 1/|x-y| and 1/|x-y|^3
+ * serve both orders), which halves the reciprocal square roots and cuts the
+ * FMA-pipe work per pair from 8 to 5 operations. It needs one partial slot
+ * per 128-triangle tile and row (16 bytes each: ne^2/8 bytes, 0.84 GB at
+ * 81,920 triangles), allocated on its first apply. Other variants always use
+ * the CUDA cores; get reports the engine an apply in `precision` with both
+ * operators would use. No counterpart in the reference. */
 #define EB_FAR_CUDA_CORES 0
 #define EB_FAR_TENSOR_CORES 1
+#define EB_FAR_SYMMETRIC 2
 int eb_mesh_set_far_engine(eb_mesh mesh, int engine);
 int eb_mesh_get_far_engine(eb_mesh mesh, int precision, int* engine);
 /* Pipe work per well-separated quadrature pair of the fused mixed SL+DL far
