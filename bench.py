@@ -42,13 +42,6 @@ SEED = 1
 ORDER = 4
 WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L{level} "
             "({ne:,} triangles, {nv:,} vertices), quadrature index 4 (Q=7)")
-# Algorithmic FP32-pipe work of one far-cell quadrature pair of the fused SL+DL apply:
-# |x-y|^2 = |x|^2 + |y|^2 - 2x.y is 1 add + 3 FMA, the SL term 1 FMA, the DL term s/r^3 is
-# 2 mul + 1 FMA: 8 FMA-pipe operations, counted as 2 flops each (the unit of the FFMA peak),
-# plus 1 MUFU reciprocal square root. Both pipes bound the kernel.
-FMA_OPS_PER_PAIR = 8
-FLOPS_PER_PAIR = 2 * FMA_OPS_PER_PAIR
-RSQRT_PER_PAIR = 1
 # DRAM bytes (read + write) of one CUDA-core far-field launch on the L6 workload under the
 # plan of 512 work items per SM (the autotuner's choice there), from an ncu capture of that
 # launch: 46.94 MB read (records, target tables) + 107.84 MB written (the partial sums of
@@ -82,7 +75,7 @@ def parse_args(argv=None):
     p.add_argument("--requests", type=int, default=2000, help="serve: number of requests in the stream")
     p.add_argument("--serve-sample", type=int, default=300,
                    help="matvec: requests of the serving stream replayed for the p50/p99 sample (0: skip)")
-    p.add_argument("--far-engine", default="cuda", choices=list(ENGINES),
+    p.add_argument("--far-engine", default="sym", choices=list(ENGINES),
                    help="matvec: far field of the mixed apply on the FP32 pipes over every ordered pair (cuda), "
                         "over every unordered pair once, added to both rows (sym), or with tcgen05 distance "
                         "GEMMs (tensor); the other engines are timed beside it")
@@ -299,7 +292,7 @@ def batch_record(local, solves=True):
         return a.elapsed_time(b) / k
 
     out = {}
-    for key, prec, engine in (("mixed", "mixed", "cuda"), ("mixed_sym", "mixed", "sym"),
+    for key, prec, engine in (("mixed", "mixed", "sym"), ("mixed_cuda", "mixed", "cuda"),
                               ("mixed_tensor", "mixed", "tensor"), ("fp64", "fp64", "cuda")):
         for m in ms:
             m.set_far_engine(engine)
@@ -310,7 +303,7 @@ def batch_record(local, solves=True):
         out[key + "_vq"] = (torch.cat(d_v).cpu().numpy(), torch.cat(d_q).cpu().numpy())
         bt.close()
     for m in ms:
-        m.set_far_engine("cuda")
+        m.set_far_engine("sym")
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     mixed_vs_fp64 = {"sl": rel(out["mixed_vq"][0], out["fp64_vq"][0]), "dl": rel(out["mixed_vq"][1], out["fp64_vq"][1])}
     # sampled rows of 8 meshes against the CPU oracle
@@ -327,8 +320,8 @@ def batch_record(local, solves=True):
     err = {"fp64_sl": rel(cat(ev, 0), cat(ev, 2)), "mixed_sl": rel(cat(ev, 1), cat(ev, 2)),
            "fp64_dl": rel(cat(eq, 0), cat(eq, 2)), "mixed_dl": rel(cat(eq, 1), cat(eq, 2)), "oracle_rows": 64,
            "mixed_vs_fp64_full": mixed_vs_fp64,
-           "mixed_sym_vs_fp64_full": {"sl": rel(out["mixed_sym_vq"][0], out["fp64_vq"][0]),
-                                      "dl": rel(out["mixed_sym_vq"][1], out["fp64_vq"][1])}}
+           "mixed_cuda_cores_vs_fp64_full": {"sl": rel(out["mixed_cuda_vq"][0], out["fp64_vq"][0]),
+                                             "dl": rel(out["mixed_cuda_vq"][1], out["fp64_vq"][1])}}
     # 4 SL right-hand sides per mesh (the Dirichlet data of the solves)
     rhs = [m.dirichlet_rhs(np.stack([1.0 / np.linalg.norm(it["nodes"] - p, axis=1) for p in it["sources"]]))
            for m, it in zip(ms, items)]
@@ -341,10 +334,10 @@ def batch_record(local, solves=True):
     rec = {"workload": "256 ellipsoids (icosphere L2-L5, 320-20,480 triangles), SL+DL batched apply "
                        "(one density pair per mesh), 4-RHS SL batched apply, GMRES(50)-IR to 1e-8",
            "quad_pairs_per_apply": int(pairs), "mesh_setup_s": t_create,
-           "sl_dl_mixed": out["mixed"], "sl_dl_mixed_symmetric": out["mixed_sym"],
+           "sl_dl_mixed": out["mixed"], "sl_dl_mixed_cuda_cores": out["mixed_cuda"],
            "sl_dl_mixed_tensor_cores": out["mixed_tensor"], "sl_dl_fp64": out["fp64"],
            "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
-           "mixed_symmetric_over_fp64": out["mixed_sym"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
+           "mixed_cuda_cores_over_fp64": out["mixed_cuda"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "mixed_tensor_cores_over_fp64": out["mixed_tensor"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "rel_err_vs_oracle": err,
            "sl_4rhs_mixed": {"ms_per_apply": ms4, "Gpairs_per_s": pairs / (ms4 * 1e-3) / 1e9,
@@ -385,48 +378,46 @@ def large_record(local, solve=False):
     t_create = time.perf_counter() - t0
     m.set_profiling(True)
     res = {}
-    for prec, engine in (("mixed_cuda", "cuda"), ("fp64", "cuda"), ("mixed", "tensor"), ("mixed_sym", "sym")):
+    for key, engine in (("mixed", "sym"), ("mixed_cuda", "cuda"), ("mixed_tensor", "tensor"), ("fp64", "cuda")):
         m.set_far_engine(engine)
-        p = "fp64" if prec == "fp64" else "mixed"
+        p = "fp64" if key == "fp64" else "mixed"
         m.apply_sl_dl(t, u, precision=p)
         v, q = m.apply_sl_dl(t, u, precision=p)
         far, fin = m.last_kernel_ms()
-        res[prec] = (v, q, far, fin)
+        res[key] = (v, q, far, fin)
+    m.set_far_engine("sym")
     rng = np.random.default_rng(5)
     rows = np.sort(rng.choice(elems.shape[0], 16, replace=False)).astype(np.int32)
     vo, qo = Oracle(ORDER).apply_rows(nodes, elems, t, u, rows)
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     pairs = m.far_quad_pairs
     peak_tflops, peak_rsqrt = _measure_peak()
-    rate_t = pairs / (res["mixed"][2] * 1e-3)  # tensor-core engine
-    mufu_pp, fma_pp, _ = _engine_costs("tensor")
-    bound_t = min(peak_tflops * 1e12 / (2 * fma_pp), peak_rsqrt * 1e12 / mufu_pp)
-    rate = pairs / (res["mixed_cuda"][2] * 1e-3)  # CUDA cores: the default engine
-    bound = min(peak_tflops * 1e12 / FLOPS_PER_PAIR, peak_rsqrt * 1e12 / RSQRT_PER_PAIR)
+
+    def engine_rec(key, engine):
+        mufu_pp, fma_pp, _ = _engine_costs(engine)
+        rate = pairs / (res[key][2] * 1e-3)
+        bound = min(peak_tflops * 1e12 / (2 * fma_pp), peak_rsqrt * 1e12 / mufu_pp)
+        return {"engine": engine, "kernel": ENGINE_KERNELS[engine], "far_ms": res[key][2],
+                "finalize_ms": res[key][3], "Gpairs_per_s": rate / 1e9,
+                "fma_pipe_frac": rate * 2 * fma_pp / (peak_tflops * 1e12),
+                "mufu_frac": rate * mufu_pp / (peak_rsqrt * 1e12), "frac_of_pair_bound": rate / bound,
+                "rel_err_sl": rel(res[key][0][rows], vo), "rel_err_dl": rel(res[key][1][rows], qo)}
+
     cf, cn = m.cell_pairs()
     rec = {"workload": "radius-perturbed icosphere L7 (327,680 triangles, 163,842 vertices)",
            "quad_pairs_per_step": pairs, "near_pairs": m.near_pairs, "mesh_setup_s": t_create,
            "near_cell_share": cn / (cf + cn),
-           "mixed": {"engine": "cuda", "far_ms": res["mixed_cuda"][2], "finalize_ms": res["mixed_cuda"][3],
-                     "Gpairs_per_s": rate / 1e9, "fma_pipe_frac": rate * FLOPS_PER_PAIR / (peak_tflops * 1e12),
-                     "frac_of_pair_bound": rate / bound},
-           "mixed_tensor_cores": {"far_ms": res["mixed"][2], "Gpairs_per_s": rate_t / 1e9,
-                                  "mufu_frac": rate_t * mufu_pp / (peak_rsqrt * 1e12),
-                                  "frac_of_pair_bound": rate_t / bound_t,
-                                  "rel_err_sl": rel(res["mixed"][0][rows], vo),
-                                  "rel_err_dl": rel(res["mixed"][1][rows], qo)},
-           "mixed_symmetric": {"far_ms": res["mixed_sym"][2], "finalize_ms": res["mixed_sym"][3],
-                               "Gpairs_per_s": pairs / (res["mixed_sym"][2] * 1e-3) / 1e9,
-                               "rel_err_sl": rel(res["mixed_sym"][0][rows], vo),
-                               "rel_err_dl": rel(res["mixed_sym"][1][rows], qo)},
+           "mixed": engine_rec("mixed", "sym"),
+           "mixed_cuda_cores": engine_rec("mixed_cuda", "cuda"),
+           "mixed_tensor_cores": engine_rec("mixed_tensor", "tensor"),
            "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
                     "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
-           "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed_cuda"][0][rows], vo),
-                                 "mixed_dl": rel(res["mixed_cuda"][1][rows], qo),
+           "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed"][0][rows], vo),
+                                 "mixed_dl": rel(res["mixed"][1][rows], qo),
                                  "fp64_sl": rel(res["fp64"][0][rows], vo), "fp64_dl": rel(res["fp64"][1][rows], qo),
                                  "oracle_rows": len(rows)}}
     rec["mixed_over_fp64"] = rec["mixed"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
-    rec["mixed_symmetric_over_fp64"] = rec["mixed_symmetric"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
+    rec["mixed_cuda_cores_over_fp64"] = rec["mixed_cuda_cores"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
     if solve:
         g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
         b = m.dirichlet_rhs(g)

@@ -190,7 +190,7 @@ class Mesh:
         """Far-field engine of the fused mixed SL+DL apply: "tensor" (tcgen05
         GEMMs for the pair distances), "cuda" (FP32 pipes only, every ordered
         pair) or "sym" (FP32 pipes, every unordered pair once, added to both
-        rows)."""
+        rows; the default)."""
         check(lib().eb_mesh_set_far_engine(self._h, FAR_ENGINES[engine]))
 
     def far_engine(self, precision="mixed"):

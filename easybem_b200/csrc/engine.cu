@@ -664,8 +664,10 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
 
 bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd)
 {
+  // the partial slots take ne^2 / 8 bytes: meshes above kSymMaxTriangles keep
+  // the CUDA-core kernel (whose slots grow with the work split, not with ne^2)
   return m->plan.engine == 2 && fp32 && nsl == 1 && nd == 1 && m->h.Q == kSymRule && m->h.K == kSymRule &&
-         m->h.nchunk == 1;
+         m->h.nchunk == 1 && m->h.ne <= kSymMaxTriangles;
 }
 
 int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd)

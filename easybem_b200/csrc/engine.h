@@ -88,7 +88,7 @@ struct DevBuf {
 
 // Launch plan of the far field for one mesh (tile shape and work split).
 struct FarPlan {
-  int engine = 0;         // 0: CUDA-core far kernel; 1: tensor-core kernel, 2: symmetric kernel, where the variant has one
+  int engine = 2;         // 0: CUDA-core far kernel; 1: tensor-core kernel, 2: symmetric kernel, where the variant has one
   int items_per_sm = 32;  // work items per SM the source ranges are cut into (load balance)
   int tile = 0;           // source triangles per shared-memory tile (0: the variant's default)
   int src_tile = kTS;     // tile of the last launch

@@ -47,6 +47,10 @@
 #ifndef EB_SYM_UNROLL_B
 #define EB_SYM_UNROLL_B 0
 #endif
+// Source cells per upper work item (even; 256 source triangles by default).
+#ifndef EB_SYM_CELLS
+#define EB_SYM_CELLS 8
+#endif
 
 namespace eb {
 
@@ -64,6 +68,7 @@ static_assert(kTS == 2 * kCell, "a staged tile is two cells");
 static_assert(kPairs * 4 == kTT, "one reduction output per thread");
 
 __device__ __forceinline__ float2 bcast(float v) { return make_float2(v, v); }
+
 
 // One target triangle (kQ points, relative to the cell centre) against the
 // source triangles [s0, s1) of one cell of the staged pair-interleaved tile,
@@ -405,7 +410,7 @@ int far_sym_occupancy()
 int far_sym_items(int nitems, int ncells, int cells_per_item, std::vector<WorkItem>& items)
 {
   const int ntt = (nitems + kTT - 1) / kTT;
-  const int r = std::max(2, cells_per_item & ~1);
+  const int r = std::max(2, (cells_per_item > 0 ? cells_per_item : EB_SYM_CELLS) & ~1);
   items.clear();
   int nsplit = 0;
   std::vector<WorkItem> diag;

@@ -12,8 +12,12 @@
 namespace eb {
 
 constexpr int kSymRule = 7;  // the engine's quadrature rule size (index 4)
-// source cells per upper work item by default (256 source triangles)
-constexpr int kSymCellsPerItem = 8;
+// source cells per upper work item: 0 takes the build's default (8 cells,
+// 256 source triangles)
+constexpr int kSymCellsPerItem = 0;
+// largest mesh the symmetric engine takes: its partial slots (one FP64 pair
+// per 128-triangle tile and row) stay at or below 2^35 bytes (32 GiB)
+constexpr int kSymMaxTriangles = 524288;
 
 // Work list of the symmetric plan for nitems = ne target rows (one item per
 // triangle) and ncells cells; returns the number of partial slots per row.

@@ -350,9 +350,12 @@ int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit
  * serve both orders), which halves the reciprocal square roots and cuts the
  * FMA-pipe work per pair from 8 to 5 operations. It needs one partial slot
  * per 128-triangle tile and row (16 bytes each: ne^2/8 bytes, 0.84 GB at
- * 81,920 triangles), allocated on its first apply. Other variants always use
- * the CUDA cores; get reports the engine an apply in `precision` with both
- * operators would use. No counterpart in the reference. */
+ * 81,920 triangles, 13.4 GB at 327,680), allocated on its first apply, and
+ * takes meshes of up to 524,288 triangles (32 GiB of slots); larger meshes
+ * use the CUDA cores. EB_FAR_SYMMETRIC is the default of a new mesh. Other
+ * variants always use the CUDA cores; get reports the engine an apply in
+ * `precision` with both operators would use. No counterpart in the
+ * reference. */
 #define EB_FAR_CUDA_CORES 0
 #define EB_FAR_TENSOR_CORES 1
 #define EB_FAR_SYMMETRIC 2
