@@ -293,7 +293,8 @@ def batch_record(local, solves=True):
 
     out = {}
     for key, prec, engine in (("mixed", "mixed", "sym"), ("mixed_cuda", "mixed", "cuda"),
-                              ("mixed_tensor", "mixed", "tensor"), ("fp64", "fp64", "cuda")):
+                              ("mixed_tensor", "mixed", "tensor"), ("fp64", "fp64", "cuda"),
+                              ("fp64_sym", "fp64", "sym_all")):
         for m in ms:
             m.set_far_engine(engine)
         bt = eb.Batch(ms, precision=prec, sl_dl=True)
@@ -336,6 +337,8 @@ def batch_record(local, solves=True):
            "quad_pairs_per_apply": int(pairs), "mesh_setup_s": t_create,
            "sl_dl_mixed": out["mixed"], "sl_dl_mixed_cuda_cores": out["mixed_cuda"],
            "sl_dl_mixed_tensor_cores": out["mixed_tensor"], "sl_dl_fp64": out["fp64"],
+           "sl_dl_fp64_symmetric": out["fp64_sym"],
+           "mixed_over_fp64_symmetric": out["mixed"]["Gpairs_per_s"] / out["fp64_sym"]["Gpairs_per_s"],
            "mixed_over_fp64": out["mixed"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "mixed_cuda_cores_over_fp64": out["mixed_cuda"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
            "mixed_tensor_cores_over_fp64": out["mixed_tensor"]["Gpairs_per_s"] / out["fp64"]["Gpairs_per_s"],
@@ -378,9 +381,10 @@ def large_record(local, solve=False):
     t_create = time.perf_counter() - t0
     m.set_profiling(True)
     res = {}
-    for key, engine in (("mixed", "sym"), ("mixed_cuda", "cuda"), ("mixed_tensor", "tensor"), ("fp64", "cuda")):
+    for key, engine in (("mixed", "sym"), ("mixed_cuda", "cuda"), ("mixed_tensor", "tensor"), ("fp64", "cuda"),
+                        ("fp64_sym", "sym_all")):
         m.set_far_engine(engine)
-        p = "fp64" if key == "fp64" else "mixed"
+        p = "fp64" if key.startswith("fp64") else "mixed"
         m.apply_sl_dl(t, u, precision=p)
         v, q = m.apply_sl_dl(t, u, precision=p)
         far, fin = m.last_kernel_ms()
@@ -412,12 +416,17 @@ def large_record(local, solve=False):
            "mixed_tensor_cores": engine_rec("mixed_tensor", "tensor"),
            "fp64": {"far_ms": res["fp64"][2], "finalize_ms": res["fp64"][3],
                     "Gpairs_per_s": pairs / (res["fp64"][2] * 1e-3) / 1e9},
+           "fp64_symmetric": {"far_ms": res["fp64_sym"][2], "finalize_ms": res["fp64_sym"][3],
+                              "Gpairs_per_s": pairs / (res["fp64_sym"][2] * 1e-3) / 1e9,
+                              "rel_err_sl": rel(res["fp64_sym"][0][rows], vo),
+                              "rel_err_dl": rel(res["fp64_sym"][1][rows], qo)},
            "rel_err_vs_oracle": {"mixed_sl": rel(res["mixed"][0][rows], vo),
                                  "mixed_dl": rel(res["mixed"][1][rows], qo),
                                  "fp64_sl": rel(res["fp64"][0][rows], vo), "fp64_dl": rel(res["fp64"][1][rows], qo),
                                  "oracle_rows": len(rows)}}
     rec["mixed_over_fp64"] = rec["mixed"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
     rec["mixed_cuda_cores_over_fp64"] = rec["mixed_cuda_cores"]["Gpairs_per_s"] / rec["fp64"]["Gpairs_per_s"]
+    rec["mixed_over_fp64_symmetric"] = rec["mixed"]["Gpairs_per_s"] / rec["fp64_symmetric"]["Gpairs_per_s"]
     if solve:
         g = 1.0 / np.linalg.norm(nodes - np.array([0.0, 0.0, 3.0]), axis=1)
         b = m.dirichlet_rhs(g)
@@ -562,6 +571,12 @@ def main():
     ms_fp64, far_fp64 = timed("fp64", k64, 1)
     v_64 = d_v.cpu().numpy()
     q_64 = d_q.cpu().numpy()
+    # FP64 on the symmetric kernel too (opt-in engine): the same formulation in both precisions
+    mesh.set_far_engine("sym_all")
+    ms_fp64s, far_fp64s = timed("fp64", k64, 1)
+    v_64s = d_v.cpu().numpy()
+    q_64s = d_q.cpu().numpy()
+    mesh.set_far_engine(args.far_engine)
     # the other far-field engines of the mixed apply, same plan
     others = {}
     for other in ENGINES:
@@ -574,8 +589,10 @@ def main():
 
     step_ms = max_over_ranks(sum(ms_mixed) / len(ms_mixed), dist, dev)
     step_ms64 = max_over_ranks(sum(ms_fp64) / len(ms_fp64), dist, dev)
+    step_ms64s = max_over_ranks(sum(ms_fp64s) / len(ms_fp64s), dist, dev)
     value = replica_throughput(world, pairs, step_ms)
     value64 = replica_throughput(world, pairs, step_ms64)
+    value64s = replica_throughput(world, pairs, step_ms64s)
 
     # e2e through the host-buffer C ABI with pinned host memory
     h_t = torch.from_numpy(t).pin_memory()
@@ -657,6 +674,12 @@ def main():
         "fp64": {"value": value64, "unit": "Gpairs/s", "ms_per_step": step_ms64, "steps": len(ms_fp64),
                  "far_ms": sum(f for f, _ in far_fp64) / len(far_fp64)},
         "mixed_over_fp64": value / value64,
+        "fp64_symmetric": {"value": value64s, "unit": "Gpairs/s", "ms_per_step": step_ms64s,
+                           "far_ms": sum(f for f, _ in far_fp64s) / len(far_fp64s),
+                           "rel_err_vs_oracle": {"sl": rel(v_64s[rows], vo), "dl": rel(q_64s[rows], qo)},
+                           "note": "the FP64 apply on the symmetric kernel (opt-in EB_FAR_SYMMETRIC_ALL); the "
+                                   "'fp64' record is the plain ordered-pair FP64 kernel, the FP64 default"},
+        "mixed_over_fp64_symmetric": value / value64s,
         "far_engine": args.far_engine,
         "other_engines": {e: {"ms_per_step": sum(o[0]) / len(o[0]),
                               "far_ms": sum(f for f, _ in o[1]) / len(o[1]),

@@ -27,7 +27,7 @@ __all__ = ["Mesh", "Batch", "Solver", "Server", "solve", "EasyBemError", "init_g
 
 
 # far-field engines of the fused mixed SL+DL apply (EB_FAR_* in easybem_gpu.h)
-FAR_ENGINES = {"cuda": 0, "tensor": 1, "sym": 2}
+FAR_ENGINES = {"cuda": 0, "tensor": 1, "sym": 2, "sym_all": 3}
 
 
 def precision_code(precision) -> int:
@@ -190,13 +190,14 @@ class Mesh:
         """Far-field engine of the fused mixed SL+DL apply: "tensor" (tcgen05
         GEMMs for the pair distances), "cuda" (FP32 pipes only, every ordered
         pair) or "sym" (FP32 pipes, every unordered pair once, added to both
-        rows; the default)."""
+        rows; the default); "sym_all" takes the symmetric kernel for the FP64
+        apply too."""
         check(lib().eb_mesh_set_far_engine(self._h, FAR_ENGINES[engine]))
 
     def far_engine(self, precision="mixed"):
         e = ctypes.c_int()
         check(lib().eb_mesh_get_far_engine(self._h, precision_code(precision), ctypes.byref(e)))
-        return {v: k for k, v in FAR_ENGINES.items()}[e.value]
+        return {v: k for k, v in FAR_ENGINES.items() if k != "sym_all"}[e.value]
 
     def set_profiling(self, on: bool = True):
         check(lib().eb_set_profiling(self._h, 1 if on else 0))

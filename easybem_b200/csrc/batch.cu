@@ -56,7 +56,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   const int n = (int)entries.size();
   tc_ = fp32 && nsl_ == 1 && nd_ == 1;
   for (BatchEntry* be : entries) tc_ = tc_ && tc_eligible(be->mesh, fp32, 1, 1);
-  sym_ = fp32 && nsl_ == 1 && nd_ == 1 && !tc_;
+  sym_ = nsl_ == 1 && nd_ == 1 && !tc_;
   for (BatchEntry* be : entries) sym_ = sym_ && sym_eligible(be->mesh, fp32, 1, 1);
   std::vector<TcPrepArgs> targs;
   std::vector<int> toff(1, 0);
@@ -167,7 +167,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     occ_ = 1;
   }
   if (sym_) {
-    occ_ = std::max(1, far_sym_occupancy());
+    occ_ = std::max(1, far_sym_occupancy(fp32));
     grid_ = std::min(nsm * occ_, std::max(1, nitems_));
   }
   return EB_OK;
@@ -196,7 +196,8 @@ int Batch::run(cudaStream_t st, int reserve_sms)
     EB_CUDA(far_tc_launch(desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(),
                           tc_err_.as<int>(), grid, st));
   else if (sym_)
-    EB_CUDA(far_sym_launch(desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(), grid, st));
+    EB_CUDA(far_sym_launch(fp32_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(), grid,
+                           st));
   else
     EB_CUDA(far_launch(fp32_, nsl_, nd_, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
                        counter_.as<int>(), smem_, grid, st));

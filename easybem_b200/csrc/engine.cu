@@ -666,8 +666,9 @@ bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd)
 {
   // the partial slots take ne^2 / 8 bytes: meshes above kSymMaxTriangles keep
   // the CUDA-core kernel (whose slots grow with the work split, not with ne^2)
-  return m->plan.engine == 2 && fp32 && nsl == 1 && nd == 1 && m->h.Q == kSymRule && m->h.K == kSymRule &&
-         m->h.nchunk == 1 && m->h.ne <= kSymMaxTriangles;
+  const bool engine = (m->plan.engine == 2 && fp32) || m->plan.engine == 3;
+  return engine && nsl == 1 && nd == 1 && m->h.Q == kSymRule && m->h.K == kSymRule && m->h.nchunk == 1 &&
+         m->h.ne <= kSymMaxTriangles;
 }
 
 int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd)
@@ -682,7 +683,7 @@ int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd)
 
 // The symmetric far field: work list and zeroed partial slots once per mesh,
 // the descriptor once per scratch allocation, then the persistent kernel.
-static int sym_far_apply(Mesh* m, cudaStream_t st)
+static int sym_far_apply(Mesh* m, bool fp32, cudaStream_t st)
 {
   const HostMesh& h = m->h;
   if (!m->sym_partial.p) {
@@ -701,16 +702,17 @@ static int sym_far_apply(Mesh* m, cudaStream_t st)
     EB_CHECK(copy_h2d(m->sym_var.desc.p, &desc, sizeof desc));
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-    const int occ = std::max(1, far_sym_occupancy());
-    m->sym_var.grid = std::min(nsm * occ, std::max(1, m->sym_nitems));
-    m->sym_var.smem = far_sym_smem_bytes();
+    m->sym_var.grid = nsm;  // times the kernel's CTAs per SM, per precision below
     m->sym_var.src_tile = kTS;
   }
+  const int occ = std::max(1, far_sym_occupancy(fp32));
+  const int grid = std::min(m->sym_var.grid * occ, std::max(1, m->sym_nitems));
+  m->sym_var.smem = far_sym_smem_bytes(fp32);
   EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev0, st));
-  EB_CUDA(far_sym_launch(m->sym_var.desc.as<FarMeshDesc>(), m->sym_items.as<WorkItem>(), m->sym_nitems,
-                         m->counter.as<int>(), m->sym_var.grid, st));
-  m->plan.grid = m->sym_var.grid;
+  EB_CUDA(far_sym_launch(fp32, m->sym_var.desc.as<FarMeshDesc>(), m->sym_items.as<WorkItem>(), m->sym_nitems,
+                         m->counter.as<int>(), grid, st));
+  m->plan.grid = grid;
   m->tc_used = false;
   m->sym_used = true;
   return EB_OK;
@@ -820,7 +822,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const
     EB_CUDA(cudaEventCreate(&m->ev2));
   }
   if (sym) {
-    EB_CHECK(sym_far_apply(m, st));
+    EB_CHECK(sym_far_apply(m, fp32, st));
     A.partial = m->sym_partial.as<double>();
     A.nsplit = m->sym_nsplit;
   } else if (tc_eligible(m, fp32, nsl, nd)) {
@@ -1118,8 +1120,10 @@ int eb_evaluate_potential(eb_mesh mesh, int precision, int npts, const double* p
 int eb_mesh_set_far_engine(eb_mesh mesh, int engine)
 {
   if (!mesh) return set_error(EB_ERR_INVALID, "null mesh");
-  if (engine != EB_FAR_CUDA_CORES && engine != EB_FAR_TENSOR_CORES && engine != EB_FAR_SYMMETRIC)
-    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES, EB_FAR_TENSOR_CORES or EB_FAR_SYMMETRIC");
+  if (engine != EB_FAR_CUDA_CORES && engine != EB_FAR_TENSOR_CORES && engine != EB_FAR_SYMMETRIC &&
+      engine != EB_FAR_SYMMETRIC_ALL)
+    return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES, EB_FAR_TENSOR_CORES, EB_FAR_SYMMETRIC or "
+                                     "EB_FAR_SYMMETRIC_ALL");
   mesh->m->plan.engine = engine;
   return EB_OK;
 }

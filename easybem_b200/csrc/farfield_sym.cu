@@ -47,6 +47,10 @@
 #ifndef EB_SYM_UNROLL_B
 #define EB_SYM_UNROLL_B 0
 #endif
+// Source-point unroll of the FP64 symmetric loop (0: full).
+#ifndef EB_SYM_UNROLL_B64
+#define EB_SYM_UNROLL_B64 0
+#endif
 // Source cells per upper work item (even; 256 source triangles by default).
 #ifndef EB_SYM_CELLS
 #define EB_SYM_CELLS 8
@@ -63,6 +67,10 @@ constexpr int kPairs = kTS / 2;              // source-triangle pairs per staged
 constexpr int kRedStride = kPairs + 1;       // float4 per thread row of the reduction buffer (padded)
 constexpr size_t kRecBytes = (size_t)kTS * kQ * kNrec * 16;
 constexpr size_t kRedBytes = (size_t)kTT * kRedStride * 16;
+constexpr int kRed64Stride = kCell + 1;      // double2 per thread row of the FP64 reduction buffer (padded)
+constexpr size_t kRec64Bytes = (size_t)kCell * kQ * kNrec * 32;
+constexpr size_t kRed64Bytes = (size_t)kTT * kRed64Stride * 16;
+constexpr int kUnrollB64 = EB_SYM_UNROLL_B64 > 0 ? EB_SYM_UNROLL_B64 : kQ;
 static_assert(kTT == 4 * kCell, "a target tile is four cells");
 static_assert(kTS == 2 * kCell, "a staged tile is two cells");
 static_assert(kPairs * 4 == kTT, "one reduction output per thread");
@@ -381,29 +389,256 @@ __global__ void __launch_bounds__(kTT, 2)
   }
 }
 
+// FP64 form of eval_cell_sym (one source triangle at a time, the arithmetic
+// of the FP64 ordered-pair kernel's eval_cell): the transposed sums of
+// triangle s go to red[s - s0] as (SL, DL).
+template <bool FAR>
+__device__ __forceinline__ void eval_cell_sym64(const dq* __restrict__ srec, const int4* __restrict__ svid,
+                                                const dq* __restrict__ snrm, const dq* __restrict__ splane, int s0,
+                                                int s1, int4 tv, const double (&x)[kQ], const double (&y)[kQ],
+                                                const double (&z)[kQ], const double (&q2)[kQ],
+                                                const double (&ca)[kQ], const double (&cd)[kQ],
+                                                const double (&wq)[kQ], const double (&o)[3], const double (&cen)[3],
+                                                const double (&nrm)[3], const double (&cc)[3], double pin,
+                                                double (&sl)[kQ], double (&dl)[kQ], double2* __restrict__ red)
+{
+  double ex = 0.0, ey = 0.0, ez = 0.0, ew = 0.0;
+  if constexpr (FAR) {
+    ex = -0.5 * nrm[0];
+    ey = -0.5 * nrm[1];
+    ez = -0.5 * nrm[2];
+    ew = cc[0] * nrm[0] + cc[1] * nrm[1] + cc[2] * nrm[2] - pin;
+  }
+#pragma unroll 1
+  for (int s = s0; s < s1; ++s) {
+    dq nj;
+    if constexpr (!FAR) {
+      if (shares_vertex(tv, svid[s])) {
+        red[s - s0] = make_double2(0.0, 0.0);
+        continue;
+      }
+      nj = snrm[s];
+      const double dnx = nrm[0] - nj.x, dny = nrm[1] - nj.y, dnz = nrm[2] - nj.z;
+      ex = -0.5 * dnx;
+      ey = -0.5 * dny;
+      ez = -0.5 * dnz;
+      ew = (nj.w - pin) + (cc[0] * dnx + cc[1] * dny + cc[2] * dnz);
+    }
+    const dq* r = srec + (size_t)s * kQ * kNrec;
+    double acc[kQ];
+#pragma unroll
+    for (int a = 0; a < kQ; ++a) acc[a] = 0.0;
+    double S = 0.0, Qt = 0.0;
+#pragma unroll(kUnrollB64)
+    for (int b = 0; b < kQ; ++b) {
+      const dq p0 = r[b * kNrec];
+      const dq p1 = r[b * kNrec + 1];  // (s_b, c_b, 0, 0)
+      double ts = 0.0, td = 0.0;
+#pragma unroll
+      for (int a = 0; a < kQ; ++a) {
+        double r2;
+        if constexpr (FAR) {
+          r2 = x[a] * p0.x + (y[a] * p0.y + (z[a] * p0.z + (q2[a] + p0.w)));
+        } else {
+          const double dx = x[a] + 0.5 * p0.x, dy = y[a] + 0.5 * p0.y, dz = z[a] + 0.5 * p0.z;
+          r2 = dx * dx + dy * dy + dz * dz;
+        }
+        const double inv = rsq_f64(r2);
+        const double inv3 = (inv * inv) * inv;
+        sl[a] += p1.y * inv;
+        acc[a] += p1.x * inv3;
+        ts += ca[a] * inv;
+        td += cd[a] * inv3;
+      }
+      const double e = p0.x * ex + (p0.y * ey + (p0.z * ez + ew));
+      S += wq[b] * ts;
+      Qt += (wq[b] * e) * td;
+    }
+    red[s - s0] = make_double2(S, Qt);
+    // forward double layer (as eval_cell)
+    if constexpr (FAR) {
+      const dq pn = splane[s];
+#pragma unroll
+      for (int a = 0; a < kQ; ++a) dl[a] += (x[a] * pn.x + (y[a] * pn.y + (z[a] * pn.z - pn.w))) * acc[a];
+    } else {
+      const double dnx = nj.x - nrm[0], dny = nj.y - nrm[1], dnz = nj.z - nrm[2];
+      const double e0 = (cen[0] * nj.x + cen[1] * nj.y + cen[2] * nj.z - nj.w) + (o[0] * dnx + (o[1] * dny + o[2] * dnz));
+#pragma unroll
+      for (int a = 0; a < kQ; ++a) dl[a] += (x[a] * dnx + (y[a] * dny + (z[a] * dnz + e0))) * acc[a];
+    }
+  }
+}
+
+// FP64 symmetric far field: the FP32 kernel's work list and slots; source
+// tiles of one cell (kCell triangles, FP64 records), the transposed sums
+// reduced per cell over the 128 target threads in FP64.
+__global__ void __launch_bounds__(kTT, 2)
+    far_sym64_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
+                     int* __restrict__ counter)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_item;
+  __shared__ int4 s_vid[kCell];
+  __shared__ dq s_nrm[kCell];
+  __shared__ dq s_plane[kCell];
+  dq* s_rec = reinterpret_cast<dq*>(smem_raw);
+  double2* s_red = reinterpret_cast<double2*>(smem_raw + kRec64Bytes);
+  double2* my_red = s_red + threadIdx.x * kRed64Stride;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= nitems) break;
+    const WorkItem w = items[it];
+    const FarMeshDesc md = meshes[w.mesh];
+    if (md.active && *md.active == 0) continue;  // uniform across the CTA
+    const bool upper = w.cell0 * kCell >= w.tgt0 + kTT;
+    const int tslot = w.tgt0 / kTT;
+    const int ti = w.tgt0 + threadIdx.x;
+    const bool active = ti < md.nitems;
+    const int tsel = active ? ti : w.tgt0;
+    const dq tile = md.twarp[tsel / kWarpItems];
+    double cen[3], nrm[3];
+    {
+      const dq c = md.tcent[tsel];
+      cen[0] = c.x; cen[1] = c.y; cen[2] = c.z;
+      const dq n = md.tnrm[tsel];
+      nrm[0] = n.x; nrm[1] = n.y; nrm[2] = n.z;
+    }
+    const double pin = md.snrm[tsel].w;
+    const int4 tv = active ? md.tvid[tsel] : make_int4(-1, -1, -1, 0);
+    const dq* grec = reinterpret_cast<const dq*>(md.rec);
+    double acc_sl = 0.0, acc_dl = 0.0;
+    const size_t stride = (size_t)md.nsplit * md.nitems;
+
+    for (int cell = w.cell0; cell < w.cell1; ++cell) {
+      const int t0 = cell * kCell;
+      const int ns = min(kCell, md.ne - t0);
+      {
+        const dq* g = grec + (size_t)t0 * kQ * kNrec;
+        const int nstage = ns * kQ * kNrec;
+        for (int k = threadIdx.x; k < nstage; k += kTT) s_rec[k] = g[k];
+        for (int k = threadIdx.x; k < ns; k += kTT) {
+          s_vid[k] = md.svid[t0 + k];
+          s_nrm[k] = md.snrm[t0 + k];
+          s_plane[k] = md.splane64[t0 + k];
+        }
+      }
+      __syncthreads();
+      if (active) {
+        const dq ccd = md.ccent[cell];
+        const double ddx = ccd.x - tile.x, ddy = ccd.y - tile.y, ddz = ccd.z - tile.z;
+        const double rr = kFarRatio * (ccd.w + tile.w);
+        const bool far = ddx * ddx + ddy * ddy + ddz * ddz > rr * rr;
+        const double o[3] = {ccd.x - cen[0], ccd.y - cen[1], ccd.z - cen[2]};
+        double xs[kQ], ys[kQ], zs[kQ], q2[kQ], wq[kQ];
+#pragma unroll
+        for (int a = 0; a < kQ; ++a) {
+          const dq p = md.tgt64[(size_t)tsel * kQ + a];
+          xs[a] = p.x - o[0]; ys[a] = p.y - o[1]; zs[a] = p.z - o[2];
+          q2[a] = xs[a] * xs[a] + ys[a] * ys[a] + zs[a] * zs[a];
+          wq[a] = p.w;
+        }
+        double sl[kQ], dl[kQ];
+#pragma unroll
+        for (int a = 0; a < kQ; ++a) { sl[a] = 0.0; dl[a] = 0.0; }
+        if (upper) {
+          double ca[kQ], cd[kQ];
+#pragma unroll
+          for (int a = 0; a < kQ; ++a) {
+            const dq st = grec[((size_t)tsel * kQ + a) * kNrec + 1];  // (s_a, c_a, 0, 0)
+            cd[a] = st.x;
+            ca[a] = st.y;
+          }
+          const double cc[3] = {ccd.x, ccd.y, ccd.z};
+          if (far)
+            eval_cell_sym64<true>(s_rec, s_vid, s_nrm, s_plane, 0, ns, tv, xs, ys, zs, q2, ca, cd, wq, o, cen, nrm,
+                                  cc, pin, sl, dl, my_red);
+          else
+            eval_cell_sym64<false>(s_rec, s_vid, s_nrm, s_plane, 0, ns, tv, xs, ys, zs, q2, ca, cd, wq, o, cen, nrm,
+                                   cc, pin, sl, dl, my_red);
+        } else {
+          double slc[1][kQ], dlc[1][kQ];
+#pragma unroll
+          for (int a = 0; a < kQ; ++a) { slc[0][a] = 0.0; dlc[0][a] = 0.0; }
+          if (far)
+            eval_cell<double, kQ, kQ, 1, 1, true>(s_rec, s_vid, s_nrm, s_plane, 0, ns, kQ, tv, xs, ys, zs, q2, o, cen,
+                                                  nrm, slc, dlc);
+          else
+            eval_cell<double, kQ, kQ, 1, 1, false>(s_rec, s_vid, s_nrm, s_plane, 0, ns, kQ, tv, xs, ys, zs, q2, o,
+                                                   cen, nrm, slc, dlc);
+#pragma unroll
+          for (int a = 0; a < kQ; ++a) { sl[a] = slc[0][a]; dl[a] = dlc[0][a]; }
+        }
+        double ps = 0.0, pd = 0.0;
+#pragma unroll
+        for (int a = 0; a < kQ; ++a) {
+          ps += wq[a] * sl[a];
+          pd += wq[a] * dl[a];
+        }
+        acc_sl += ps;
+        acc_dl += pd;
+      } else if (upper) {
+        for (int k = 0; k < kCell; ++k) my_red[k] = make_double2(0.0, 0.0);
+      }
+      if (upper) {
+        // thread t < 2 kCell adds output t % 2 of source triangle t / 2 over
+        // the 128 target threads in order
+        __syncthreads();
+        const int k = threadIdx.x >> 1, c = threadIdx.x & 1;
+        if (threadIdx.x < 2 * kCell && k < ns) {
+          const double* rf = reinterpret_cast<const double*>(s_red) + 2 * k + c;
+          double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+#pragma unroll 8
+          for (int t = 0; t < kTT; t += 4) {
+            v0 += rf[(t + 0) * kRed64Stride * 2];
+            v1 += rf[(t + 1) * kRed64Stride * 2];
+            v2 += rf[(t + 2) * kRed64Stride * 2];
+            v3 += rf[(t + 3) * kRed64Stride * 2];
+          }
+          md.partial[c * stride + (size_t)tslot * md.nitems + t0 + k] = (v0 + v1) + (v2 + v3);
+        }
+      }
+      __syncthreads();
+    }
+    if (active) {
+      double* out = md.partial + (size_t)w.split * md.nitems + ti;
+      out[0] = acc_sl;
+      out[stride] = acc_dl;
+    }
+  }
+}
+
 }  // namespace
 
-size_t far_sym_smem_bytes() { return kRecBytes + kRedBytes; }
+size_t far_sym_smem_bytes(bool fp32) { return fp32 ? kRecBytes + kRedBytes : kRec64Bytes + kRed64Bytes; }
 
-cudaError_t far_sym_launch(const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, int grid, cudaStream_t st)
+cudaError_t far_sym_launch(bool fp32, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, int grid,
+                           cudaStream_t st)
 {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(far_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)far_sym_smem_bytes());
+  // the attribute is per device: set it on every launch (a host-side call)
+  const size_t smem = far_sym_smem_bytes(fp32);
+  if (fp32) {
+    cudaError_t e = cudaFuncSetAttribute(far_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    attr = true;
+    far_sym_kernel<<<grid, kTT, smem, st>>>(dm, di, n, dc);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(far_sym64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    far_sym64_kernel<<<grid, kTT, smem, st>>>(dm, di, n, dc);
   }
-  far_sym_kernel<<<grid, kTT, far_sym_smem_bytes(), st>>>(dm, di, n, dc);
   return cudaGetLastError();
 }
 
-int far_sym_occupancy()
+int far_sym_occupancy(bool fp32)
 {
   int occ = 0;
-  cudaFuncSetAttribute(far_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)far_sym_smem_bytes());
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, far_sym_kernel, kTT, far_sym_smem_bytes()) != cudaSuccess)
-    return 0;
+  const size_t smem = far_sym_smem_bytes(fp32);
+  const void* fn = fp32 ? (const void*)far_sym_kernel : (const void*)far_sym64_kernel;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kTT, smem) != cudaSuccess) return 0;
   return occ;
 }
 

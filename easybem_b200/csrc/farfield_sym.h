@@ -22,10 +22,12 @@ constexpr int kSymMaxTriangles = 524288;
 // Work list of the symmetric plan for nitems = ne target rows (one item per
 // triangle) and ncells cells; returns the number of partial slots per row.
 int far_sym_items(int nitems, int ncells, int cells_per_item, std::vector<WorkItem>& items);
-// Dynamic shared memory of one CTA (staged tile + transposed-sum buffer).
-size_t far_sym_smem_bytes();
+// Dynamic shared memory of one CTA (staged tile + transposed-sum buffer) of
+// the FP32 (fp32) or FP64 kernel.
+size_t far_sym_smem_bytes(bool fp32);
 // Resident CTAs per SM.
-int far_sym_occupancy();
-cudaError_t far_sym_launch(const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, int grid, cudaStream_t st);
+int far_sym_occupancy(bool fp32);
+cudaError_t far_sym_launch(bool fp32, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, int grid,
+                           cudaStream_t st);
 
 }  // namespace eb

@@ -9,7 +9,7 @@ the sampled rows of the whole batch and per mesh) and against the
 single-mesh fused apply (rounding only: the batch's shared-memory tile is
 the smallest of its meshes'), with the far field on the CUDA cores and, for
 the mixed apply, on the tensor cores and on the symmetric engine (every
-unordered pair once).
+unordered pair once; in FP64 too).
 """
 import numpy as np
 import pytest
@@ -45,7 +45,7 @@ def test_batched_sl_dl_matches_oracle_on_sampled_rows(gpu_lib, batch40, oracle):
         ref_q.append(qo)
         rows.append(r)
     for prec, tol, engine in (("fp64", 1e-12, "cuda"), ("mixed", 1e-6, "cuda"), ("mixed", 1e-6, "tensor"),
-                              ("mixed", 1e-6, "sym")):
+                              ("mixed", 1e-6, "sym"), ("fp64", 1e-12, "sym_all")):
         for m in ms:
             m.set_far_engine(engine)
         bt = gpu_lib.Batch(ms, precision=prec, sl_dl=True)
@@ -63,7 +63,7 @@ def test_batched_sl_dl_matches_oracle_on_sampled_rows(gpu_lib, batch40, oracle):
 def test_batched_sl_dl_equals_single_mesh_applies(gpu_lib, batch40):
     items, ms, ts, us = batch40
     for prec, tol, engine in (("fp64", 1e-14, "cuda"), ("mixed", 1e-7, "cuda"), ("mixed", 1e-7, "tensor"),
-                              ("mixed", 1e-7, "sym")):
+                              ("mixed", 1e-7, "sym"), ("fp64", 1e-14, "sym_all")):
         for m in ms:
             m.set_far_engine(engine)
         bt = gpu_lib.Batch(ms, precision=prec, sl_dl=True)

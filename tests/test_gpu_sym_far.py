@@ -9,7 +9,8 @@ small meshes whose every cell is near (masks, the direct-difference form,
 the per-lane plane distance), an open surface, two components, and larger
 meshes where most cells are well separated. Results are bitwise
 reproducible: every partial slot is written by one work item and folded in
-slot order.
+slot order. The FP64 form (EB_FAR_SYMMETRIC_ALL, opt-in) is held to the FP64
+bar (1e-12 against the oracle).
 """
 import numpy as np
 import pytest
@@ -103,3 +104,26 @@ def test_symmetric_far_field_follows_plan_changes(gpu_lib):
             v, q = m.apply_sl_dl(t, u, precision="mixed")
             # the symmetric work list does not depend on the forward plan
             assert np.array_equal(v, v0) and np.array_equal(q, q0), ips
+
+
+def test_symmetric_far_field_in_fp64(gpu_lib, golden_ops, oracle):
+    oracle.set_order(4)
+    for name, nodes, elems in _cases(golden_ops)[3:]:
+        rng = np.random.default_rng(len(name) + 7)
+        t = rng.normal(size=elems.shape[0])
+        u = rng.normal(size=nodes.shape[0])
+        ne = elems.shape[0]
+        rows = np.arange(ne) if ne <= 1280 else np.sort(rng.choice(ne, 96, replace=False))
+        vo, qo = oracle.apply_rows(nodes, elems, t, u, rows.astype(np.int32))
+        with gpu_lib.Mesh(nodes, elems) as m:
+            v0, q0 = m.apply_sl_dl(t, u)  # the plain ordered-pair FP64 kernel (the default)
+            m.set_far_engine("sym_all")
+            assert m.far_engine("fp64") == "sym" and m.far_engine("mixed") == "sym"
+            v, q = m.apply_sl_dl(t, u)
+            v2, q2 = m.apply_sl_dl(t, u)
+            print(f"{name} ({ne} triangles): symmetric FP64 SL {rel_l2(v[rows], vo):.2e} DL {rel_l2(q[rows], qo):.2e}")
+            assert rel_l2(v[rows], vo) < 1e-12 and rel_l2(q[rows], qo) < 1e-12, name
+            assert rel_l2(v, v0) < 1e-13 and rel_l2(q, q0) < 1e-13, name
+            assert np.array_equal(v, v2) and np.array_equal(q, q2), name
+            vm, qm = m.apply_sl_dl(t, u, precision="mixed")
+            assert rel_l2(vm[rows], vo) < MIXED_TOL and rel_l2(qm[rows], qo) < MIXED_TOL, name
