@@ -1148,9 +1148,10 @@ int eb_far_engine_costs(int engine, double* mufu_per_pair, double* fma_ops_per_p
     if (tensor_flops_per_pair) *tensor_flops_per_pair = 0.0;
   } else if (engine == EB_FAR_SYMMETRIC) {
     // one evaluation per unordered pair, i.e. per two ordered pairs: 1 MUFU,
-    // |x-y|^2 1 add + 3 FMA, r^3 2 mul, 4 FMA for the SL and DL sums of both orders
+    // |x-y|^2 1 add + 3 FMA, r^3 2 mul, 1 FMA for the SL sum both rows share,
+    // 2 FMA for the DL sums of both rows
     if (mufu_per_pair) *mufu_per_pair = 0.5;
-    if (fma_ops_per_pair) *fma_ops_per_pair = 5.0;
+    if (fma_ops_per_pair) *fma_ops_per_pair = 4.5;
     if (tensor_flops_per_pair) *tensor_flops_per_pair = 0.0;
   } else {
     return set_error(EB_ERR_INVALID, "engine must be EB_FAR_CUDA_CORES, EB_FAR_TENSOR_CORES or EB_FAR_SYMMETRIC");

@@ -267,6 +267,11 @@ __device__ __forceinline__ void prep_point(const ApplyArgs& A, long long idx)
 #pragma unroll
   for (int c = 0; c < NSL; ++c)
     vals[4 * charge_slot(c, ND) + charge_comp(c, ND)] = (T)(wj * A.t[(size_t)c * A.tstride + orig]);
+  if constexpr (NSL == 1 && ND == 1) {
+    // the triangle's SL charge without the point weight, J_j t_j (the
+    // symmetric far field factors c_b = w_b J_j t_j)
+    vals[6] = (T)(A.trin[j].w * A.t[orig]);
+  }
   if constexpr (ND > 0) {
     const int4 v = A.svid[j];
     const double e1 = A.bary[2 * b], e2 = A.bary[2 * b + 1];

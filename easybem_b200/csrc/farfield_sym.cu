@@ -13,9 +13,11 @@
 // with c = w J t the SL charges and s = w J u_h the DL strengths of the
 // points, d_j(x) = (x - P0_j).n_j the signed distance of x from the plane of
 // triangle j and e_i(y) = (y - P0_i).n_i that of y from the plane of i. Each
-// unordered pair is evaluated once: one MUFU rsqrt and 10 FMA-pipe lane
-// operations (1 add + 3 FMA for |x - y|^2, 2 mul for r^3, 4 FMA for the four
-// sums) instead of 2 rsqrt and 16 for the two ordered pairs.
+// unordered pair is evaluated once: one MUFU rsqrt and 9 FMA-pipe lane
+// operations (1 add + 3 FMA for |x - y|^2, 2 mul for r^3, 1 FMA for the
+// single-layer sum R_a = sum_b w_b r that both rows share, 2 FMA for the
+// double-layer sums of the two rows) instead of 2 rsqrt and 16 for the two
+// ordered pairs.
 //
 // Work items of the symmetric plan (tiles of kTT = 128 sorted triangles, cells
 // of kCell = 32):
@@ -80,10 +82,16 @@ __device__ __forceinline__ float2 bcast(float v) { return make_float2(v, v); }
 
 // One target triangle (kQ points, relative to the cell centre) against the
 // source triangles [s0, s1) of one cell of the staged pair-interleaved tile,
-// both orders of every pair. Forward sums go to sl/dl (per target point, as
-// eval_cell_sp); the transposed sums of source triangles s, s+1 go to
-// red[s / 2] as (SL s, SL s+1, DL s, DL s+1), already weighted by the source
-// points' rule weights w_b (the finalize multiplies a row by J / 4 pi).
+// both orders of every pair. Forward sums: the single layer as one sum
+// already weighted by the target points' rule weights (slw), the double
+// layer per target point (dl, as eval_cell_sp); the transposed sums of
+// source triangles s, s+1 go to red[s / 2] as (SL s, SL s+1, DL s, DL s+1),
+// weighted by the source points' rule weights w_b (the finalize multiplies a
+// row by J / 4 pi).
+//
+// Single layer: both charges factor as c = w J t, so one sum per target
+// point, R_a = sum_b w_b / r_ab, serves both rows: row i gets J_j t_j
+// sum_a w_a R_a, row j gets sum_a c_a R_a (1 FMA per pair instead of 2).
 //
 // Far cells: expanded |x - y|^2 and e_i(y) = (y - c).n_i + (c - P0_i).n_i;
 // other cells: direct differences, a 1e-24 floor and, per lane, e_i(y) =
@@ -98,17 +106,17 @@ __device__ __forceinline__ void eval_cell_sym(const float4* __restrict__ srec, c
                                               const float (&z)[kQ], const float (&q2)[kQ], const float (&ca)[kQ],
                                               const float (&cd)[kQ], const float (&wq)[kQ], const float (&o)[3],
                                               const double (&cen)[3], const double (&nrm)[3],
-                                              const double (&cc)[3], double pin, float (&sl)[kQ], float (&dl)[kQ],
+                                              const double (&cc)[3], double pin, float& slw, float (&dl)[kQ],
                                               float4* __restrict__ red)
 {
-  float2 X[kQ], Y[kQ], Z[kQ], W[kQ], SL[kQ], DLp[kQ];
+  float2 X[kQ], Y[kQ], Z[kQ], W[kQ], DLp[kQ];
+  float2 SLW = make_float2(0.f, 0.f);
 #pragma unroll
   for (int a = 0; a < kQ; ++a) {
     X[a] = bcast(x[a]);
     Y[a] = bcast(y[a]);
     Z[a] = bcast(z[a]);
     W[a] = bcast(q2[a]);
-    SL[a] = make_float2(0.f, 0.f);
     DLp[a] = make_float2(0.f, 0.f);
   }
   const float2 half2 = bcast(0.5f);
@@ -147,20 +155,23 @@ __device__ __forceinline__ void eval_cell_sym(const float4* __restrict__ srec, c
       EW = make_float2(e[0][3], e[1][3]);
     }
     const float4* r = srec + (size_t)(s >> 1) * kQ * kNrec * 2;
-    float2 acc2[kQ];
+    float2 tj = sp_comp(r, 1, 2);  // J_j t_j of both triangles
+    if constexpr (!FAR) tj = __fmul2_rn(tj, keep);
+    float2 acc2[kQ], R[kQ];
 #pragma unroll
-    for (int a = 0; a < kQ; ++a) acc2[a] = make_float2(0.f, 0.f);
-    float2 S2 = make_float2(0.f, 0.f), Q2 = make_float2(0.f, 0.f);
+    for (int a = 0; a < kQ; ++a) {
+      acc2[a] = make_float2(0.f, 0.f);
+      R[a] = make_float2(0.f, 0.f);
+    }
+    float2 Q2 = make_float2(0.f, 0.f);
 #pragma unroll(kUnrollB)
     for (int b = 0; b < kQ; ++b) {
       const float4* rv = r + b * kNrec * 2;
       const float2 px = sp_comp(rv, 0, 0), py = sp_comp(rv, 0, 1), pz = sp_comp(rv, 0, 2), pw = sp_comp(rv, 0, 3);
-      float2 sd = sp_comp(rv, 1, 0), ch = sp_comp(rv, 1, 1);
-      if constexpr (!FAR) {
-        sd = __fmul2_rn(sd, keep);
-        ch = __fmul2_rn(ch, keep);
-      }
-      float2 ts = make_float2(0.f, 0.f), td = make_float2(0.f, 0.f);
+      float2 sd = sp_comp(rv, 1, 0);
+      if constexpr (!FAR) sd = __fmul2_rn(sd, keep);
+      const float2 wb = bcast(wq[b]);
+      float2 td = make_float2(0.f, 0.f);
 #pragma unroll
       for (int a = 0; a < kQ; ++a) {
         float2 r2;
@@ -174,19 +185,23 @@ __device__ __forceinline__ void eval_cell_sym(const float4* __restrict__ srec, c
         }
         const float2 inv = make_float2(rsq(r2.x), rsq(r2.y));
         const float2 inv3 = __fmul2_rn(__fmul2_rn(inv, inv), inv);
-        SL[a] = __ffma2_rn(ch, inv, SL[a]);
+        R[a] = __ffma2_rn(wb, inv, R[a]);
         acc2[a] = __ffma2_rn(sd, inv3, acc2[a]);
-        ts.x = fmaf(ca[a], inv.x, ts.x);
-        ts.y = fmaf(ca[a], inv.y, ts.y);
         td.x = fmaf(cd[a], inv3.x, td.x);
         td.y = fmaf(cd[a], inv3.y, td.y);
       }
       // e_i(y_b) for both lanes; y_b - c = -(1/2)(-2 y_b)
       const float2 e = __ffma2_rn(px, EX, __ffma2_rn(py, EY, __ffma2_rn(pz, EZ, EW)));
-      const float2 wb = bcast(wq[b]);
-      S2 = __ffma2_rn(wb, ts, S2);
       Q2 = __ffma2_rn(__fmul2_rn(wb, e), td, Q2);
     }
+    // single layer of both rows from R_a
+    float2 U = make_float2(0.f, 0.f), S2 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < kQ; ++a) {
+      U = __ffma2_rn(bcast(wq[a]), R[a], U);
+      S2 = __ffma2_rn(bcast(ca[a]), R[a], S2);
+    }
+    SLW = __ffma2_rn(tj, U, SLW);
     if constexpr (!FAR) {
       S2 = __fmul2_rn(S2, keep);
       Q2 = __fmul2_rn(Q2, keep);
@@ -222,11 +237,9 @@ __device__ __forceinline__ void eval_cell_sym(const float4* __restrict__ srec, c
       DLp[a] = __ffma2_rn(d, acc2[a], DLp[a]);
     }
   }
+  slw += SLW.x + SLW.y;
 #pragma unroll
-  for (int a = 0; a < kQ; ++a) {
-    sl[a] += SL[a].x + SL[a].y;
-    dl[a] += DLp[a].x + DLp[a].y;
-  }
+  for (int a = 0; a < kQ; ++a) dl[a] += DLp[a].x + DLp[a].y;
 }
 
 __global__ void __launch_bounds__(kTT, 2)
@@ -316,7 +329,7 @@ __global__ void __launch_bounds__(kTT, 2)
             q2[a] = xs[a] * xs[a] + ys[a] * ys[a] + zs[a] * zs[a];
             wq[a] = p.w;
           }
-          float sl[kQ], dl[kQ];
+          float sl[kQ], dl[kQ], slw = 0.f;
 #pragma unroll
           for (int a = 0; a < kQ; ++a) { sl[a] = 0.f; dl[a] = 0.f; }
           if (upper) {
@@ -330,10 +343,10 @@ __global__ void __launch_bounds__(kTT, 2)
             const double cc[3] = {ccd.x, ccd.y, ccd.z};
             if (far)
               eval_cell_sym<true>(s_rec, s_vid, s_nrm, s_plane, g0, g1, tv, xs, ys, zs, q2, ca, cd, wq, o, cen, nrm,
-                                  cc, pin, sl, dl, my_red);
+                                  cc, pin, slw, dl, my_red);
             else
               eval_cell_sym<false>(s_rec, s_vid, s_nrm, s_plane, g0, g1, tv, xs, ys, zs, q2, ca, cd, wq, o, cen,
-                                   nrm, cc, pin, sl, dl, my_red);
+                                   nrm, cc, pin, slw, dl, my_red);
           } else {
             float slc[1][kQ], dlc[1][kQ];
 #pragma unroll
@@ -347,7 +360,7 @@ __global__ void __launch_bounds__(kTT, 2)
 #pragma unroll
             for (int a = 0; a < kQ; ++a) { sl[a] = slc[0][a]; dl[a] = dlc[0][a]; }
           }
-          float ps = 0.f, pd = 0.f;
+          float ps = slw, pd = 0.f;  // slw: the symmetric form's weighted SL sum (0 on the diagonal)
 #pragma unroll
           for (int a = 0; a < kQ; ++a) {
             ps += wq[a] * sl[a];
@@ -390,8 +403,8 @@ __global__ void __launch_bounds__(kTT, 2)
 }
 
 // FP64 form of eval_cell_sym (one source triangle at a time, the arithmetic
-// of the FP64 ordered-pair kernel's eval_cell): the transposed sums of
-// triangle s go to red[s - s0] as (SL, DL).
+// of the FP64 ordered-pair kernel's eval_cell, the single layer through
+// R_a): the transposed sums of triangle s go to red[s - s0] as (SL, DL).
 template <bool FAR>
 __device__ __forceinline__ void eval_cell_sym64(const dq* __restrict__ srec, const int4* __restrict__ svid,
                                                 const dq* __restrict__ snrm, const dq* __restrict__ splane, int s0,
@@ -400,7 +413,7 @@ __device__ __forceinline__ void eval_cell_sym64(const dq* __restrict__ srec, con
                                                 const double (&ca)[kQ], const double (&cd)[kQ],
                                                 const double (&wq)[kQ], const double (&o)[3], const double (&cen)[3],
                                                 const double (&nrm)[3], const double (&cc)[3], double pin,
-                                                double (&sl)[kQ], double (&dl)[kQ], double2* __restrict__ red)
+                                                double& slw, double (&dl)[kQ], double2* __restrict__ red)
 {
   double ex = 0.0, ey = 0.0, ez = 0.0, ew = 0.0;
   if constexpr (FAR) {
@@ -425,15 +438,19 @@ __device__ __forceinline__ void eval_cell_sym64(const dq* __restrict__ srec, con
       ew = (nj.w - pin) + (cc[0] * dnx + cc[1] * dny + cc[2] * dnz);
     }
     const dq* r = srec + (size_t)s * kQ * kNrec;
-    double acc[kQ];
+    const double tj = r[1].z;  // J_j t_j
+    double acc[kQ], R[kQ];
 #pragma unroll
-    for (int a = 0; a < kQ; ++a) acc[a] = 0.0;
-    double S = 0.0, Qt = 0.0;
+    for (int a = 0; a < kQ; ++a) {
+      acc[a] = 0.0;
+      R[a] = 0.0;
+    }
+    double Qt = 0.0;
 #pragma unroll(kUnrollB64)
     for (int b = 0; b < kQ; ++b) {
       const dq p0 = r[b * kNrec];
-      const dq p1 = r[b * kNrec + 1];  // (s_b, c_b, 0, 0)
-      double ts = 0.0, td = 0.0;
+      const dq p1 = r[b * kNrec + 1];  // (s_b, c_b, J_j t_j, 0)
+      double td = 0.0;
 #pragma unroll
       for (int a = 0; a < kQ; ++a) {
         double r2;
@@ -445,15 +462,20 @@ __device__ __forceinline__ void eval_cell_sym64(const dq* __restrict__ srec, con
         }
         const double inv = rsq_f64(r2);
         const double inv3 = (inv * inv) * inv;
-        sl[a] += p1.y * inv;
+        R[a] += wq[b] * inv;
         acc[a] += p1.x * inv3;
-        ts += ca[a] * inv;
         td += cd[a] * inv3;
       }
       const double e = p0.x * ex + (p0.y * ey + (p0.z * ez + ew));
-      S += wq[b] * ts;
       Qt += (wq[b] * e) * td;
     }
+    double U = 0.0, S = 0.0;
+#pragma unroll
+    for (int a = 0; a < kQ; ++a) {
+      U += wq[a] * R[a];
+      S += ca[a] * R[a];
+    }
+    slw += tj * U;
     red[s - s0] = make_double2(S, Qt);
     // forward double layer (as eval_cell)
     if constexpr (FAR) {
@@ -541,7 +563,7 @@ __global__ void __launch_bounds__(kTT, 2)
           q2[a] = xs[a] * xs[a] + ys[a] * ys[a] + zs[a] * zs[a];
           wq[a] = p.w;
         }
-        double sl[kQ], dl[kQ];
+        double sl[kQ], dl[kQ], slw = 0.0;
 #pragma unroll
         for (int a = 0; a < kQ; ++a) { sl[a] = 0.0; dl[a] = 0.0; }
         if (upper) {
@@ -555,10 +577,10 @@ __global__ void __launch_bounds__(kTT, 2)
           const double cc[3] = {ccd.x, ccd.y, ccd.z};
           if (far)
             eval_cell_sym64<true>(s_rec, s_vid, s_nrm, s_plane, 0, ns, tv, xs, ys, zs, q2, ca, cd, wq, o, cen, nrm,
-                                  cc, pin, sl, dl, my_red);
+                                  cc, pin, slw, dl, my_red);
           else
             eval_cell_sym64<false>(s_rec, s_vid, s_nrm, s_plane, 0, ns, tv, xs, ys, zs, q2, ca, cd, wq, o, cen, nrm,
-                                   cc, pin, sl, dl, my_red);
+                                   cc, pin, slw, dl, my_red);
         } else {
           double slc[1][kQ], dlc[1][kQ];
 #pragma unroll
@@ -572,7 +594,7 @@ __global__ void __launch_bounds__(kTT, 2)
 #pragma unroll
           for (int a = 0; a < kQ; ++a) { sl[a] = slc[0][a]; dl[a] = dlc[0][a]; }
         }
-        double ps = 0.0, pd = 0.0;
+        double ps = slw, pd = 0.0;  // slw: the symmetric form's weighted SL sum (0 on the diagonal)
 #pragma unroll
         for (int a = 0; a < kQ; ++a) {
           ps += wq[a] * sl[a];

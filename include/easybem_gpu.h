@@ -348,7 +348,7 @@ int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit
  * pair once on the FP32 pipes and adds it to both rows of its triangle pair
  * (the test and trial rules are the same rule, so 1/|x-y| and 1/|x-y|^3
  * serve both orders), which halves the reciprocal square roots and cuts the
- * FMA-pipe work per pair from 8 to 5 operations. It needs one partial slot
+ * FMA-pipe work per pair from 8 to 4.5 operations. It needs one partial slot
  * per 128-triangle tile and row (16 bytes each: ne^2/8 bytes, 0.84 GB at
  * 81,920 triangles, 13.4 GB at 327,680), allocated on its first apply, and
  * takes meshes of up to 524,288 triangles (32 GiB of slots); larger meshes
@@ -360,7 +360,7 @@ int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit
 #define EB_FAR_TENSOR_CORES 1
 #define EB_FAR_SYMMETRIC 2
 /* EB_FAR_SYMMETRIC for the FP64 fused SL+DL apply too (every unordered pair
- * once in FP64: 7.5 instead of 13 FP64-pipe operations per pair). Opt-in:
+ * once in FP64: 7 instead of 13 FP64-pipe operations per pair). Opt-in:
  * the FP64 default stays the plain ordered-pair kernel; get reports
  * EB_FAR_SYMMETRIC for an FP64 apply on this engine. */
 #define EB_FAR_SYMMETRIC_ALL 3
