@@ -56,8 +56,8 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   const int n = (int)entries.size();
   tc_ = fp32 && nsl_ == 1 && nd_ == 1;
   for (BatchEntry* be : entries) tc_ = tc_ && tc_eligible(be->mesh, fp32, 1, 1);
-  sym_ = nsl_ == 1 && nd_ == 1 && !tc_;
-  for (BatchEntry* be : entries) sym_ = sym_ && sym_eligible(be->mesh, fp32, 1, 1);
+  sym_ = !tc_;
+  for (BatchEntry* be : entries) sym_ = sym_ && sym_eligible(be->mesh, fp32, nsl_, nd_);
   std::vector<TcPrepArgs> targs;
   std::vector<int> toff(1, 0);
   std::vector<FarMeshDesc> desc(n);
@@ -91,7 +91,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     int sym_nsplit = 0;
     if (sym_) {  // the mesh's symmetric work list and its own zeroed partial slots
       sym_nsplit = far_sym_items(h.nitems, h.ncells, kSymCellsPerItem, sym_items);
-      const size_t bytes = sizeof(double) * 2 * (size_t)sym_nsplit * h.nitems;
+      const size_t bytes = sizeof(double) * (size_t)(nsl_ + nd_) * (size_t)sym_nsplit * h.nitems;
       if (be->sym_partial.bytes < bytes) {
         be->sym_partial.release();
         EB_CHECK(be->sym_partial.alloc(bytes));
@@ -167,7 +167,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     occ_ = 1;
   }
   if (sym_) {
-    occ_ = std::max(1, far_sym_occupancy(fp32));
+    occ_ = std::max(1, far_sym_occupancy(fp32, nsl_, nd_));
     grid_ = std::min(nsm * occ_, std::max(1, nitems_));
   }
   return EB_OK;
@@ -196,8 +196,8 @@ int Batch::run(cudaStream_t st, int reserve_sms)
     EB_CUDA(far_tc_launch(desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(),
                           tc_err_.as<int>(), grid, st));
   else if (sym_)
-    EB_CUDA(far_sym_launch(fp32_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_, counter_.as<int>(), grid,
-                           st));
+    EB_CUDA(far_sym_launch(fp32_, nsl_, nd_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
+                           counter_.as<int>(), grid, st));
   else
     EB_CUDA(far_launch(fp32_, nsl_, nd_, K_, Q_, desc_.as<FarMeshDesc>(), items_.as<WorkItem>(), nitems_,
                        counter_.as<int>(), smem_, grid, st));

@@ -662,13 +662,20 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
   return desc;
 }
 
+size_t sym_slot_bytes(const HostMesh& h, int nout)
+{
+  const long long nsplit = (h.nitems + kTT - 1) / kTT + 1;  // at most one slot per tile, plus one
+  return sizeof(double) * (size_t)nout * (size_t)nsplit * (size_t)h.nitems;
+}
+
 bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd)
 {
-  // the partial slots take ne^2 / 8 bytes: meshes above kSymMaxTriangles keep
-  // the CUDA-core kernel (whose slots grow with the work split, not with ne^2)
+  // the partial slots take (nsl + nd) ne^2 / 128 * 8 bytes: meshes whose slots
+  // would pass kSymMaxSlotBytes keep the ordered-pair kernels (whose slots
+  // grow with the work split, not with ne^2)
   const bool engine = (m->plan.engine == 2 && fp32) || m->plan.engine == 3;
-  return engine && nsl == 1 && nd == 1 && m->h.Q == kSymRule && m->h.K == kSymRule && m->h.nchunk == 1 &&
-         m->h.ne <= kSymMaxTriangles;
+  return engine && far_sym_variant(fp32, nsl, nd) && m->h.Q == kSymRule && m->h.K == kSymRule &&
+         m->h.nchunk == 1 && sym_slot_bytes(m->h, nsl + nd) <= kSymMaxSlotBytes;
 }
 
 int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd)
@@ -681,16 +688,22 @@ int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd)
   return m->plan.nsplit;
 }
 
-// The symmetric far field: work list and zeroed partial slots once per mesh,
-// the descriptor once per scratch allocation, then the persistent kernel.
-static int sym_far_apply(Mesh* m, bool fp32, cudaStream_t st)
+// The symmetric far field: work list once per mesh, zeroed partial slots for
+// the widest variant used so far (grown and zeroed again when a wider one
+// comes), the descriptor once per scratch allocation, then the persistent
+// kernel.
+static int sym_far_apply(Mesh* m, bool fp32, int nsl, int nd, cudaStream_t st)
 {
   const HostMesh& h = m->h;
-  if (!m->sym_partial.p) {
+  if (!m->sym_items.p) {
     m->sym_nsplit = far_sym_items(h.nitems, h.ncells, kSymCellsPerItem, m->sym_items_host);
     m->sym_nitems = (int)m->sym_items_host.size();
     EB_CHECK(upload(m->sym_items, m->sym_items_host));
-    const size_t bytes = sizeof(double) * 2 * (size_t)m->sym_nsplit * h.nitems;
+  }
+  const size_t bytes = sizeof(double) * (size_t)(nsl + nd) * (size_t)m->sym_nsplit * h.nitems;
+  if (m->sym_partial.bytes < bytes) {
+    m->sym_partial.release();
+    m->sym_var.desc.release();
     EB_CHECK(m->sym_partial.alloc(bytes));
     EB_CUDA(cudaMemsetAsync(m->sym_partial.p, 0, bytes, st));
   }
@@ -705,13 +718,13 @@ static int sym_far_apply(Mesh* m, bool fp32, cudaStream_t st)
     m->sym_var.grid = nsm;  // times the kernel's CTAs per SM, per precision below
     m->sym_var.src_tile = kTS;
   }
-  const int occ = std::max(1, far_sym_occupancy(fp32));
+  const int occ = std::max(1, far_sym_occupancy(fp32, nsl, nd));
   const int grid = std::min(m->sym_var.grid * occ, std::max(1, m->sym_nitems));
-  m->sym_var.smem = far_sym_smem_bytes(fp32);
+  m->sym_var.smem = far_sym_smem_bytes(fp32, nsl, nd);
   EB_CUDA(cudaMemsetAsync(m->counter.p, 0, sizeof(int), st));
   if (m->profile) EB_CUDA(cudaEventRecord(m->ev0, st));
-  EB_CUDA(far_sym_launch(fp32, m->sym_var.desc.as<FarMeshDesc>(), m->sym_items.as<WorkItem>(), m->sym_nitems,
-                         m->counter.as<int>(), grid, st));
+  EB_CUDA(far_sym_launch(fp32, nsl, nd, m->sym_var.desc.as<FarMeshDesc>(), m->sym_items.as<WorkItem>(),
+                         m->sym_nitems, m->counter.as<int>(), grid, st));
   m->plan.grid = grid;
   m->tc_used = false;
   m->sym_used = true;
@@ -822,7 +835,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const
     EB_CUDA(cudaEventCreate(&m->ev2));
   }
   if (sym) {
-    EB_CHECK(sym_far_apply(m, fp32, st));
+    EB_CHECK(sym_far_apply(m, fp32, nsl, nd, st));
     A.partial = m->sym_partial.as<double>();
     A.nsplit = m->sym_nsplit;
   } else if (tc_eligible(m, fp32, nsl, nd)) {

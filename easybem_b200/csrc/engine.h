@@ -167,9 +167,12 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
 // True when mesh m applies the fused FP32 SL+DL far field with the
 // tensor-core kernel (engine 1, 7-point rule).
 bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd);
-// True when mesh m applies the fused FP32 SL+DL far field with the symmetric
-// kernel (engine 2, 7-point rule, one target item per triangle).
+// True when mesh m applies this far-field variant with a symmetric kernel
+// (engine 2 for FP32, engine 3 for both precisions; 7-point rule, one target
+// item per triangle; SL+DL, or SL only with 1, 3 or 4 columns in FP32).
 bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd);
+// Device bytes of the symmetric kernels' partial slots for nout outputs.
+size_t sym_slot_bytes(const HostMesh& h, int nout);
 // Partial slots per row of the far field the next apply in `precision` with
 // nsl SL and nd DL columns would fold.
 int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd);

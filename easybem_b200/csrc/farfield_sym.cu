@@ -633,32 +633,291 @@ __global__ void __launch_bounds__(kTT, 2)
   }
 }
 
-}  // namespace
-
-size_t far_sym_smem_bytes(bool fp32) { return fp32 ? kRecBytes + kRedBytes : kRec64Bytes + kRed64Bytes; }
-
-cudaError_t far_sym_launch(bool fp32, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, int grid,
-                           cudaStream_t st)
+// Single-layer-only symmetric far field with NC right-hand sides (FP32): the
+// batched solver's and the single-layer applies' variant. With no double
+// layer, each unordered pair costs 1 MUFU rsqrt and 5 FMA-pipe operations
+// (|x - y|^2 and R_a += (w_b / w_0) r), whatever NC: the charges of every
+// column factor as c = w J t, so the columns differ only in the per-pair
+// folds (row i: c_0 sum_a w_a R_a, with c_0 the source's first-point charge;
+// row j: sum_a w_0 c_a R_a). Every column runs the same instructions in
+// every NC, so a column's sums are the same bits alone or among 3 or 4.
+constexpr int kSlPairs = kCell / 2;  // source-triangle pairs per staged cell
+template <int NC>
+__host__ __device__ constexpr int sl_red_stride() { return kSlPairs * NC + 2; }  // float2 per thread row (padded)
+template <int NC>
+__host__ __device__ constexpr size_t sl_smem_bytes()
 {
-  // the attribute is per device: set it on every launch (a host-side call)
-  const size_t smem = far_sym_smem_bytes(fp32);
-  if (fp32) {
-    cudaError_t e = cudaFuncSetAttribute(far_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    far_sym_kernel<<<grid, kTT, smem, st>>>(dm, di, n, dc);
-  } else {
-    cudaError_t e = cudaFuncSetAttribute(far_sym64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    far_sym64_kernel<<<grid, kTT, smem, st>>>(dm, di, n, dc);
-  }
-  return cudaGetLastError();
+  return (size_t)kSlPairs * kQ * kNrec * 2 * 16 + (size_t)kTT * sl_red_stride<NC>() * 8;
 }
 
-int far_sym_occupancy(bool fp32)
+template <int NC, bool FAR>
+__device__ __forceinline__ void eval_cell_sym_sl(const float4* __restrict__ srec, const int4* __restrict__ svid,
+                                                 int s0, int s1, int4 tv, const float (&x)[kQ],
+                                                 const float (&y)[kQ], const float (&z)[kQ],
+                                                 const float (&q2)[kQ], const float (&cw)[NC][kQ],
+                                                 const float (&om)[kQ], const float (&wq)[kQ], float (&slw)[NC],
+                                                 float2* __restrict__ red)
+{
+  float2 X[kQ], Y[kQ], Z[kQ], W[kQ];
+#pragma unroll
+  for (int a = 0; a < kQ; ++a) {
+    X[a] = bcast(x[a]);
+    Y[a] = bcast(y[a]);
+    Z[a] = bcast(z[a]);
+    W[a] = bcast(q2[a]);
+  }
+  float2 SLW[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) SLW[c] = make_float2(0.f, 0.f);
+  const float2 half2 = bcast(0.5f);
+  const float2 eps2 = bcast(1e-24f);
+#pragma unroll 1
+  for (int s = s0; s < s1; s += 2) {
+    float2 keep = make_float2(1.f, 1.f);
+    if constexpr (!FAR) {
+      const bool m0 = shares_vertex(tv, svid[s]), m1 = shares_vertex(tv, svid[s + 1]);
+      if (m0 && m1) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) red[(s >> 1) * NC + c] = make_float2(0.f, 0.f);
+        continue;
+      }
+      keep = make_float2(m0 ? 0.f : 1.f, m1 ? 0.f : 1.f);
+    }
+    const float4* r = srec + (size_t)(s >> 1) * kQ * kNrec * 2;
+    float2 R[kQ];
+#pragma unroll
+    for (int a = 0; a < kQ; ++a) R[a] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int b = 0; b < kQ; ++b) {
+      const float4* rv = r + b * kNrec * 2;
+      const float2 px = sp_comp(rv, 0, 0), py = sp_comp(rv, 0, 1), pz = sp_comp(rv, 0, 2), pw = sp_comp(rv, 0, 3);
+      const float2 ob = bcast(om[b]);
+#pragma unroll
+      for (int a = 0; a < kQ; ++a) {
+        float2 r2;
+        if constexpr (FAR) {
+          r2 = __ffma2_rn(X[a], px, __ffma2_rn(Y[a], py, __ffma2_rn(Z[a], pz, __fadd2_rn(W[a], pw))));
+        } else {
+          const float2 dx = __ffma2_rn(half2, px, X[a]);
+          const float2 dy = __ffma2_rn(half2, py, Y[a]);
+          const float2 dz = __ffma2_rn(half2, pz, Z[a]);
+          r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+        }
+        const float2 inv = make_float2(rsq(r2.x), rsq(r2.y));
+        R[a] = __ffma2_rn(ob, inv, R[a]);
+      }
+    }
+    float2 U = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < kQ; ++a) U = __ffma2_rn(bcast(wq[a]), R[a], U);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      float2 c0 = sp_comp(r, 1, c);  // first-point charges of both triangles
+      if constexpr (!FAR) c0 = __fmul2_rn(c0, keep);
+      SLW[c] = __ffma2_rn(c0, U, SLW[c]);
+      float2 S = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int a = 0; a < kQ; ++a) {
+        S.x = fmaf(cw[c][a], R[a].x, S.x);
+        S.y = fmaf(cw[c][a], R[a].y, S.y);
+      }
+      if constexpr (!FAR) S = __fmul2_rn(S, keep);
+      red[(s >> 1) * NC + c] = S;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) slw[c] += SLW[c].x + SLW[c].y;
+}
+
+template <int NC>
+__global__ void __launch_bounds__(kTT, 2)
+    far_sym_sl_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
+                      int* __restrict__ counter)
+{
+  constexpr int kRow = sl_red_stride<NC>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_item;
+  __shared__ int4 s_vid[kCell];
+  float4* s_rec = reinterpret_cast<float4*>(smem_raw);
+  float2* s_red = reinterpret_cast<float2*>(smem_raw + (size_t)kSlPairs * kQ * kNrec * 2 * 16);
+  float2* my_red = s_red + threadIdx.x * kRow;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= nitems) break;
+    const WorkItem w = items[it];
+    const FarMeshDesc md = meshes[w.mesh];
+    if (md.active && *md.active == 0) continue;  // uniform across the CTA
+    const bool upper = w.cell0 * kCell >= w.tgt0 + kTT;
+    const int tslot = w.tgt0 / kTT;
+    const int ti = w.tgt0 + threadIdx.x;
+    const bool active = ti < md.nitems;
+    const int tsel = active ? ti : w.tgt0;
+    const dq tile = md.twarp[tsel / kWarpItems];
+    double cen[3];
+    {
+      const dq c = md.tcent[tsel];
+      cen[0] = c.x; cen[1] = c.y; cen[2] = c.z;
+    }
+    const int4 tv = active ? md.tvid[tsel] : make_int4(-1, -1, -1, 0);
+    const float4* grec = reinterpret_cast<const float4*>(md.rec);
+    float acc_hi[NC], acc_lo[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) { acc_hi[c] = 0.f; acc_lo[c] = 0.f; }
+    const size_t stride = (size_t)md.nsplit * md.nitems;
+
+    for (int cell = w.cell0; cell < w.cell1; ++cell) {
+      const int t0 = cell * kCell;
+      const int ns = min(kCell, md.ne - t0);
+      {  // stage the cell in the source-pair layout
+        const float4* g = grec + (size_t)t0 * kQ * kNrec;
+        constexpr int per = kQ * kNrec;
+        const int nstage = ((ns + 1) >> 1) * per;
+        for (int k = threadIdx.x; k < nstage; k += kTT) {
+          const int p = k / per, rem = k - p * per;
+          const float4 a = g[(size_t)(2 * p) * per + rem];
+          float4 c;
+          if (2 * p + 1 < ns) c = g[(size_t)(2 * p + 1) * per + rem];
+          else c = rem % kNrec == 0 ? make_float4(0.f, 0.f, 0.f, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+          s_rec[2 * k] = make_float4(a.x, c.x, a.y, c.y);
+          s_rec[2 * k + 1] = make_float4(a.z, c.z, a.w, c.w);
+        }
+        if ((ns & 1) && threadIdx.x == 0) s_vid[ns] = make_int4(-1, -1, -1, 0);
+        for (int k = threadIdx.x; k < ns; k += kTT) s_vid[k] = md.svid[t0 + k];
+      }
+      __syncthreads();
+      if (active) {
+        const dq ccd = md.ccent[cell];
+        const double ddx = ccd.x - tile.x, ddy = ccd.y - tile.y, ddz = ccd.z - tile.z;
+        const double rr = kFarRatio * (ccd.w + tile.w);
+        const bool far = ddx * ddx + ddy * ddy + ddz * ddz > rr * rr;
+        const float o[3] = {(float)(ccd.x - cen[0]), (float)(ccd.y - cen[1]), (float)(ccd.z - cen[2])};
+        float xs[kQ], ys[kQ], zs[kQ], q2[kQ], wq[kQ];
+#pragma unroll
+        for (int a = 0; a < kQ; ++a) {
+          const float4 p = md.tgt32[(size_t)tsel * kQ + a];
+          xs[a] = p.x - o[0]; ys[a] = p.y - o[1]; zs[a] = p.z - o[2];
+          q2[a] = xs[a] * xs[a] + ys[a] * ys[a] + zs[a] * zs[a];
+          wq[a] = p.w;
+        }
+        float part[NC];
+        if (upper) {
+          float cw[NC][kQ], om[kQ], slw[NC];
+#pragma unroll
+          for (int a = 0; a < kQ; ++a) {
+            om[a] = wq[a] / wq[0];
+            const float4 st = grec[((size_t)tsel * kQ + a) * kNrec + 1];  // the target's charges c_a
+#pragma unroll
+            for (int c = 0; c < NC; ++c) cw[c][a] = wq[0] * comp(st, c);
+          }
+#pragma unroll
+          for (int c = 0; c < NC; ++c) slw[c] = 0.f;
+          if (far)
+            eval_cell_sym_sl<NC, true>(s_rec, s_vid, 0, ns, tv, xs, ys, zs, q2, cw, om, wq, slw, my_red);
+          else
+            eval_cell_sym_sl<NC, false>(s_rec, s_vid, 0, ns, tv, xs, ys, zs, q2, cw, om, wq, slw, my_red);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) part[c] = slw[c];
+        } else {
+          const dq* nul = nullptr;
+          const double zero3[3] = {0.0, 0.0, 0.0};
+          float slc[NC][kQ], dlc[1][kQ];
+#pragma unroll
+          for (int a = 0; a < kQ; ++a) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) slc[c][a] = 0.f;
+            dlc[0][a] = 0.f;
+          }
+          if (far)
+            eval_cell_sp<kQ, kQ, NC, 0, true>(s_rec, s_vid, nul, nullptr, 0, ns, kQ, tv, xs, ys, zs, q2, o, cen,
+                                             zero3, slc, dlc);
+          else
+            eval_cell_sp<kQ, kQ, NC, 0, false>(s_rec, s_vid, nul, nullptr, 0, ns, kQ, tv, xs, ys, zs, q2, o, cen,
+                                              zero3, slc, dlc);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            part[c] = 0.f;
+#pragma unroll
+            for (int a = 0; a < kQ; ++a) part[c] += wq[a] * slc[c][a];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) two_sum_add(acc_hi[c], acc_lo[c], part[c]);
+      } else if (upper) {
+        for (int k = 0; k < kSlPairs * NC; ++k) my_red[k] = make_float2(0.f, 0.f);
+      }
+      if (upper) {
+        // thread t < kCell * NC adds column c, triangle 2p + l (t = (p NC + c) 2 + l)
+        // of the cell over the 128 target threads in order
+        __syncthreads();
+        const int pc = threadIdx.x >> 1, l = threadIdx.x & 1;
+        const int p = pc / NC, c = pc - p * NC;
+        if (threadIdx.x < kCell * NC && 2 * p + l < ns) {
+          const float* rf = reinterpret_cast<const float*>(s_red) + 2 * pc + l;
+          float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+#pragma unroll 8
+          for (int t = 0; t < kTT; t += 4) {
+            v0 += rf[(t + 0) * kRow * 2];
+            v1 += rf[(t + 1) * kRow * 2];
+            v2 += rf[(t + 2) * kRow * 2];
+            v3 += rf[(t + 3) * kRow * 2];
+          }
+          md.partial[c * stride + (size_t)tslot * md.nitems + t0 + 2 * p + l] = (double)((v0 + v1) + (v2 + v3));
+        }
+      }
+      __syncthreads();
+    }
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        md.partial[c * stride + (size_t)w.split * md.nitems + ti] = (double)acc_hi[c] + (double)acc_lo[c];
+    }
+  }
+}
+
+}  // namespace
+
+size_t far_sym_smem_bytes(bool fp32, int nsl, int nd)
+{
+  if (nd == 0) return nsl == 1 ? sl_smem_bytes<1>() : nsl == 3 ? sl_smem_bytes<3>() : sl_smem_bytes<4>();
+  return fp32 ? kRecBytes + kRedBytes : kRec64Bytes + kRed64Bytes;
+}
+
+static const void* sym_kernel_fn(bool fp32, int nsl, int nd)
+{
+  if (nd == 1 && nsl == 1) return fp32 ? (const void*)far_sym_kernel : (const void*)far_sym64_kernel;
+  if (nd == 0 && fp32) {
+    if (nsl == 1) return (const void*)far_sym_sl_kernel<1>;
+    if (nsl == 3) return (const void*)far_sym_sl_kernel<3>;
+    if (nsl == 4) return (const void*)far_sym_sl_kernel<4>;
+  }
+  return nullptr;
+}
+
+bool far_sym_variant(bool fp32, int nsl, int nd) { return sym_kernel_fn(fp32, nsl, nd) != nullptr; }
+
+cudaError_t far_sym_launch(bool fp32, int nsl, int nd, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc,
+                           int grid, cudaStream_t st)
+{
+  const void* fn = sym_kernel_fn(fp32, nsl, nd);
+  if (!fn) return cudaErrorInvalidValue;
+  // the attribute is per device: set it on every launch (a host-side call)
+  const size_t smem = far_sym_smem_bytes(fp32, nsl, nd);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&dm, (void*)&di, (void*)&n, (void*)&dc};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(kTT), args, smem, st);
+}
+
+int far_sym_occupancy(bool fp32, int nsl, int nd)
 {
   int occ = 0;
-  const size_t smem = far_sym_smem_bytes(fp32);
-  const void* fn = fp32 ? (const void*)far_sym_kernel : (const void*)far_sym64_kernel;
+  const void* fn = sym_kernel_fn(fp32, nsl, nd);
+  if (!fn) return 0;
+  const size_t smem = far_sym_smem_bytes(fp32, nsl, nd);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kTT, smem) != cudaSuccess) return 0;
   return occ;

@@ -15,19 +15,22 @@ constexpr int kSymRule = 7;  // the engine's quadrature rule size (index 4)
 // source cells per upper work item: 0 takes the build's default (8 cells,
 // 256 source triangles)
 constexpr int kSymCellsPerItem = 0;
-// largest mesh the symmetric engine takes: its partial slots (one FP64 pair
-// per 128-triangle tile and row) stay at or below 2^35 bytes (32 GiB)
-constexpr int kSymMaxTriangles = 524288;
+// largest slot allocation the symmetric engine takes (one FP64 value per
+// output, 128-triangle tile and row): 2^35 bytes (32 GiB), an SL+DL mesh of
+// 524,288 triangles
+constexpr size_t kSymMaxSlotBytes = (size_t)1 << 35;
 
 // Work list of the symmetric plan for nitems = ne target rows (one item per
 // triangle) and ncells cells; returns the number of partial slots per row.
 int far_sym_items(int nitems, int ncells, int cells_per_item, std::vector<WorkItem>& items);
-// Dynamic shared memory of one CTA (staged tile + transposed-sum buffer) of
-// the FP32 (fp32) or FP64 kernel.
-size_t far_sym_smem_bytes(bool fp32);
+// Variants with a symmetric kernel: SL+DL (nsl = nd = 1) in FP32 and FP64;
+// SL only with 1, 3 or 4 right-hand sides in FP32.
+bool far_sym_variant(bool fp32, int nsl, int nd);
+// Dynamic shared memory of one CTA (staged tile + transposed-sum buffer).
+size_t far_sym_smem_bytes(bool fp32, int nsl, int nd);
 // Resident CTAs per SM.
-int far_sym_occupancy(bool fp32);
-cudaError_t far_sym_launch(bool fp32, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc, int grid,
-                           cudaStream_t st);
+int far_sym_occupancy(bool fp32, int nsl, int nd);
+cudaError_t far_sym_launch(bool fp32, int nsl, int nd, const FarMeshDesc* dm, const WorkItem* di, int n, int* dc,
+                           int grid, cudaStream_t st);
 
 }  // namespace eb

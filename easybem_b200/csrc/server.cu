@@ -64,7 +64,9 @@ static size_t estimate_bytes(int nv, int ne, int order, int nrhs, int restart)
   const size_t Q = q.nt;
   const size_t mesh = (size_t)ne * (13 * (12 + 48) + 400 + Q * (16 + 32 + 8 + 16 + 32 + 3 * 32)) + (size_t)nv * 40;
   const size_t solver = (size_t)nrhs * ne * 8 * (restart + 4) + ((size_t)nrhs + 3) / 4 * ne * (Q * 64 + 160);
-  return mesh + solver;
+  // the symmetric far field's partial slots: kBatchCols outputs per 128-triangle tile and row
+  const size_t slots = (size_t)kBatchCols * (((size_t)ne + kTT - 1) / kTT + 1) * ne * 8;
+  return mesh + solver + slots;
 }
 
 struct Request {
@@ -350,7 +352,10 @@ class Server {
       }
       // replace the estimate by the measured footprint
       const size_t actual = mesh_resident_bytes(eb_mesh_internal(m)) +
-                            (size_t)r->nrhs * pool_.device_bytes_per_system(eb_mesh_internal(m));
+                            (size_t)r->nrhs * pool_.device_bytes_per_system(eb_mesh_internal(m)) +
+                            (sym_eligible(eb_mesh_internal(m), true, kBatchCols, 0)
+                                 ? sym_slot_bytes(eb_mesh_internal(m)->h, kBatchCols)
+                                 : 0);
       used_ = used_ - r->bytes + actual;
       r->bytes = actual;
       r->mesh = m;

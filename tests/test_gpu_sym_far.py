@@ -127,3 +127,41 @@ def test_symmetric_far_field_in_fp64(gpu_lib, golden_ops, oracle):
             assert np.array_equal(v, v2) and np.array_equal(q, q2), name
             vm, qm = m.apply_sl_dl(t, u, precision="mixed")
             assert rel_l2(vm[rows], vo) < MIXED_TOL and rel_l2(qm[rows], qo) < MIXED_TOL, name
+
+
+def test_symmetric_single_layer_columns(gpu_lib, oracle):
+    """The single-layer-only symmetric kernels (1, 3 and 4 right-hand sides,
+    the solver's batched applies): against the oracle and the ordered-pair
+    kernel, and every column of a 3- or 4-column batch bitwise equal to the
+    same column applied alone."""
+    import torch
+    oracle.set_order(4)
+    cases = [meshes.perturbed_icosphere(4, seed=5), meshes.torus(100, 0.3)]
+    v, f = meshes.icosphere(3)
+    cases.append((v * np.array([2.0, 0.7, 0.25]), f))
+    ms = [gpu_lib.Mesh(n, e) for n, e in cases]
+    rng = np.random.default_rng(77)
+    for (nodes, elems), m in zip(cases, ms):
+        t = rng.normal(size=elems.shape[0])
+        rows = np.sort(rng.choice(elems.shape[0], 64, replace=False)).astype(np.int32)
+        vo, _ = oracle.apply_rows(nodes, elems, t, np.zeros(nodes.shape[0]), rows)
+        m.set_far_engine("cuda")
+        vc = m.apply_sl(t, precision="mixed")
+        m.set_far_engine("sym")
+        vs = m.apply_sl(t, precision="mixed")
+        assert rel_l2(vs[rows], vo) < MIXED_TOL and rel_l2(vs, vc) < MIXED_TOL
+        assert np.array_equal(vs, m.apply_sl(t, precision="mixed"))
+    for ncols in (3, 4):
+        ts = [rng.normal(size=(ncols, m.nelems)) for m in ms]
+        d_t = [torch.from_numpy(x).cuda() for x in ts]
+        d_v = [torch.empty_like(x) for x in d_t]
+        bt = gpu_lib.Batch(ms, ncols, "mixed")
+        bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v])
+        torch.cuda.synchronize()
+        bt.close()
+        for m, t, dv in zip(ms, ts, d_v):
+            vv = dv.cpu().numpy()
+            for c in range(ncols):
+                assert np.array_equal(vv[c], m.apply_sl(t[c], precision="mixed")), (ncols, c)
+    for m in ms:
+        m.close()
