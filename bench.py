@@ -48,6 +48,9 @@ WORKLOAD = ("single-mesh SL(P0)+DL(P1) matvec, radius-perturbed icosphere L{leve
 # the 117-way source split).
 FAR_TRAFFIC_L6 = 46.94e6 + 107.84e6
 FAR_TRAFFIC_PLAN = 512
+# The same for the symmetric kernel on the L6 workload (independent of the plan): 81.45 MB
+# read + 597.83 MB written (the FP64 partial slots, one per 128-triangle tile, row and output).
+FAR_SYM_TRAFFIC_L6 = 81.45e6 + 597.83e6
 # Far-field engines of the fused mixed apply and their kernels.
 ENGINES = ("cuda", "sym", "tensor")
 ENGINE_KERNELS = {"cuda": "far_kernel<float,7,7,1,1,false>", "sym": "far_sym_kernel",
@@ -700,8 +703,9 @@ def main():
         "roofline": {"bound": ENGINE_BOUNDS[args.far_engine],
                      "achieved": pair_rate / 1e9, "peak": pair_bound / 1e9, "unit": "Gpairs/s",
                      "frac": pair_rate / pair_bound,
-                     "traffic": FAR_TRAFFIC_L6 if (args.level == LEVEL and args.far_engine == "cuda"
-                                                   and plan_info.get("items_per_sm") == FAR_TRAFFIC_PLAN) else None,
+                     "traffic": (FAR_SYM_TRAFFIC_L6 if args.level == LEVEL and args.far_engine == "sym" else
+                                 FAR_TRAFFIC_L6 if (args.level == LEVEL and args.far_engine == "cuda"
+                                                    and plan_info.get("items_per_sm") == FAR_TRAFFIC_PLAN) else None),
                      "traffic_unit": "bytes per launch",
                      "kernel": ENGINE_KERNELS[args.far_engine],
                      "far_ms": far_avg,
