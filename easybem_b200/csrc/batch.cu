@@ -40,7 +40,7 @@ void Batch::reset_graph()
 
 int batch_width(int cols) { return cols <= 1 ? 1 : (cols <= 3 ? 3 : 4); }
 
-int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags, int nd)
+int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags, int nd, bool sym_fp64)
 {
   reset_graph();
   entries_ = entries;
@@ -57,7 +57,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
   tc_ = fp32 && nsl_ == 1 && nd_ == 1;
   for (BatchEntry* be : entries) tc_ = tc_ && tc_eligible(be->mesh, fp32, 1, 1);
   sym_ = !tc_;
-  for (BatchEntry* be : entries) sym_ = sym_ && sym_eligible(be->mesh, fp32, nsl_, nd_);
+  for (BatchEntry* be : entries) sym_ = sym_ && sym_eligible(be->mesh, fp32, nsl_, nd_, sym_fp64);
   std::vector<TcPrepArgs> targs;
   std::vector<int> toff(1, 0);
   std::vector<FarMeshDesc> desc(n);

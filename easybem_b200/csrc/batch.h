@@ -38,8 +38,11 @@ class Batch {
   // quadrature order). fp32 selects the mixed-precision far field.
   // nsl: right-hand sides computed per entry (1, 3 or 4; columns beyond an
   // entry's systems carry zeros). nd = 1 adds the double layer (uin -> qout)
-  // in the same pass, with nsl 0 or 1 (the fused SL+DL variant).
-  int build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags, int nd = 0);
+  // in the same pass, with nsl 0 or 1 (the fused SL+DL variant). sym_fp64:
+  // an FP64 batch inside the library (the solver's residuals) that takes the
+  // symmetric kernels when the meshes' engine is the default.
+  int build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, int* d_flags, int nd = 0,
+            bool sym_fp64 = false);
   // One apply of all entries whose flag is set (inputs tin, outputs vout).
   // reserve_sms > 0 sizes the persistent far-field grid to leave that many
   // SMs free for kernels of other streams (the far kernel holds every SM it

@@ -668,12 +668,12 @@ size_t sym_slot_bytes(const HostMesh& h, int nout)
   return sizeof(double) * (size_t)nout * (size_t)nsplit * (size_t)h.nitems;
 }
 
-bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd)
+bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd, bool fp64_internal)
 {
   // the partial slots take (nsl + nd) ne^2 / 128 * 8 bytes: meshes whose slots
   // would pass kSymMaxSlotBytes keep the ordered-pair kernels (whose slots
   // grow with the work split, not with ne^2)
-  const bool engine = (m->plan.engine == 2 && fp32) || m->plan.engine == 3;
+  const bool engine = (m->plan.engine == 2 && (fp32 || fp64_internal)) || m->plan.engine == 3;
   return engine && far_sym_variant(fp32, nsl, nd) && m->h.Q == kSymRule && m->h.K == kSymRule &&
          m->h.nchunk == 1 && sym_slot_bytes(m->h, nsl + nd) <= kSymMaxSlotBytes;
 }

@@ -169,8 +169,10 @@ FarMeshDesc mesh_far_desc(const Mesh* m, bool fp32, int nsl, int nd, void* rec, 
 bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd);
 // True when mesh m applies this far-field variant with a symmetric kernel
 // (engine 2 for FP32, engine 3 for both precisions; 7-point rule, one target
-// item per triangle; SL+DL, or SL only with 1, 3 or 4 columns in FP32).
-bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd);
+// item per triangle; SL+DL, or SL only with 1, 3 or 4 columns).
+// fp64_internal: an FP64 apply inside the library (the solver's residuals),
+// which takes the symmetric kernel on engine 2 too.
+bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd, bool fp64_internal = false);
 // Device bytes of the symmetric kernels' partial slots for nout outputs.
 size_t sym_slot_bytes(const HostMesh& h, int nout);
 // Partial slots per row of the far field the next apply in `precision` with

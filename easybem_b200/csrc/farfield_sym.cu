@@ -878,11 +878,212 @@ __global__ void __launch_bounds__(kTT, 2)
   }
 }
 
+// FP64 single-layer-only symmetric far field (NC right-hand sides): the
+// batched solver's FP64 residual applies. The FP32 form's arithmetic in FP64,
+// one source triangle at a time; staged and reduced per half cell (16
+// triangles: the transposed buffer holds a double per column and triangle).
+constexpr int kSl64Tris = kCell / 2;
+template <int NC>
+__host__ __device__ constexpr int sl64_red_stride() { return kSl64Tris * NC + 1; }  // doubles per thread row
+template <int NC>
+__host__ __device__ constexpr size_t sl64_smem_bytes()
+{
+  return (size_t)kSl64Tris * kQ * kNrec * 32 + (size_t)kTT * sl64_red_stride<NC>() * 8;
+}
+
+template <int NC, bool FAR>
+__device__ __forceinline__ void eval_cell_sym64_sl(const dq* __restrict__ srec, const int4* __restrict__ svid, int s0,
+                                                   int s1, int4 tv, const double (&x)[kQ], const double (&y)[kQ],
+                                                   const double (&z)[kQ], const double (&q2)[kQ],
+                                                   const double (&cw)[NC][kQ], const double (&om)[kQ],
+                                                   const double (&wq)[kQ], double (&slw)[NC],
+                                                   double* __restrict__ red)
+{
+#pragma unroll 1
+  for (int s = s0; s < s1; ++s) {
+    if constexpr (!FAR) {
+      if (shares_vertex(tv, svid[s])) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) red[(s - s0) * NC + c] = 0.0;
+        continue;
+      }
+    }
+    const dq* r = srec + (size_t)s * kQ * kNrec;
+    double R[kQ];
+#pragma unroll
+    for (int a = 0; a < kQ; ++a) R[a] = 0.0;
+#pragma unroll(kUnrollB64)
+    for (int b = 0; b < kQ; ++b) {
+      const dq p0 = r[b * kNrec];
+#pragma unroll
+      for (int a = 0; a < kQ; ++a) {
+        double r2;
+        if constexpr (FAR) {
+          r2 = x[a] * p0.x + (y[a] * p0.y + (z[a] * p0.z + (q2[a] + p0.w)));
+        } else {
+          const double dx = x[a] + 0.5 * p0.x, dy = y[a] + 0.5 * p0.y, dz = z[a] + 0.5 * p0.z;
+          r2 = dx * dx + dy * dy + dz * dz;
+        }
+        R[a] += om[b] * rsq_f64(r2);
+      }
+    }
+    double U = 0.0;
+#pragma unroll
+    for (int a = 0; a < kQ; ++a) U += wq[a] * R[a];
+    const dq p1 = r[1];  // first-point charges
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      slw[c] += comp(p1, c) * U;
+      double S = 0.0;
+#pragma unroll
+      for (int a = 0; a < kQ; ++a) S += cw[c][a] * R[a];
+      red[(s - s0) * NC + c] = S;
+    }
+  }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(kTT, 2)
+    far_sym64_sl_kernel(const FarMeshDesc* __restrict__ meshes, const WorkItem* __restrict__ items, int nitems,
+                        int* __restrict__ counter)
+{
+  constexpr int kRow = sl64_red_stride<NC>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_item;
+  __shared__ int4 s_vid[kSl64Tris];
+  dq* s_rec = reinterpret_cast<dq*>(smem_raw);
+  double* s_red = reinterpret_cast<double*>(smem_raw + (size_t)kSl64Tris * kQ * kNrec * 32);
+  double* my_red = s_red + threadIdx.x * kRow;
+
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= nitems) break;
+    const WorkItem w = items[it];
+    const FarMeshDesc md = meshes[w.mesh];
+    if (md.active && *md.active == 0) continue;  // uniform across the CTA
+    const bool upper = w.cell0 * kCell >= w.tgt0 + kTT;
+    const int tslot = w.tgt0 / kTT;
+    const int ti = w.tgt0 + threadIdx.x;
+    const bool active = ti < md.nitems;
+    const int tsel = active ? ti : w.tgt0;
+    const dq tile = md.twarp[tsel / kWarpItems];
+    double cen[3];
+    {
+      const dq c = md.tcent[tsel];
+      cen[0] = c.x; cen[1] = c.y; cen[2] = c.z;
+    }
+    const int4 tv = active ? md.tvid[tsel] : make_int4(-1, -1, -1, 0);
+    const dq* grec = reinterpret_cast<const dq*>(md.rec);
+    double acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+    const size_t stride = (size_t)md.nsplit * md.nitems;
+
+    for (int half = 2 * w.cell0; half < 2 * w.cell1; ++half) {
+      const int cell = half >> 1;
+      const int t0 = half * kSl64Tris;
+      const int ns = min(kSl64Tris, md.ne - t0);
+      if (ns <= 0) break;  // uniform: the mesh's last cell has no second half
+      {
+        const dq* g = grec + (size_t)t0 * kQ * kNrec;
+        const int nstage = ns * kQ * kNrec;
+        for (int k = threadIdx.x; k < nstage; k += kTT) s_rec[k] = g[k];
+        for (int k = threadIdx.x; k < ns; k += kTT) s_vid[k] = md.svid[t0 + k];
+      }
+      __syncthreads();
+      if (active) {
+        const dq ccd = md.ccent[cell];
+        const double ddx = ccd.x - tile.x, ddy = ccd.y - tile.y, ddz = ccd.z - tile.z;
+        const double rr = kFarRatio * (ccd.w + tile.w);
+        const bool far = ddx * ddx + ddy * ddy + ddz * ddz > rr * rr;
+        const double o[3] = {ccd.x - cen[0], ccd.y - cen[1], ccd.z - cen[2]};
+        double xs[kQ], ys[kQ], zs[kQ], q2[kQ], wq[kQ];
+#pragma unroll
+        for (int a = 0; a < kQ; ++a) {
+          const dq p = md.tgt64[(size_t)tsel * kQ + a];
+          xs[a] = p.x - o[0]; ys[a] = p.y - o[1]; zs[a] = p.z - o[2];
+          q2[a] = xs[a] * xs[a] + ys[a] * ys[a] + zs[a] * zs[a];
+          wq[a] = p.w;
+        }
+        double part[NC];
+        if (upper) {
+          double cw[NC][kQ], om[kQ];
+#pragma unroll
+          for (int a = 0; a < kQ; ++a) {
+            om[a] = wq[a] / wq[0];
+            const dq st = grec[((size_t)tsel * kQ + a) * kNrec + 1];  // the target's charges c_a
+#pragma unroll
+            for (int c = 0; c < NC; ++c) cw[c][a] = wq[0] * comp(st, c);
+          }
+#pragma unroll
+          for (int c = 0; c < NC; ++c) part[c] = 0.0;
+          if (far)
+            eval_cell_sym64_sl<NC, true>(s_rec, s_vid, 0, ns, tv, xs, ys, zs, q2, cw, om, wq, part, my_red);
+          else
+            eval_cell_sym64_sl<NC, false>(s_rec, s_vid, 0, ns, tv, xs, ys, zs, q2, cw, om, wq, part, my_red);
+        } else {
+          const double zero3[3] = {0.0, 0.0, 0.0};
+          double slc[NC][kQ], dlc[1][kQ];
+#pragma unroll
+          for (int a = 0; a < kQ; ++a) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) slc[c][a] = 0.0;
+            dlc[0][a] = 0.0;
+          }
+          if (far)
+            eval_cell<double, kQ, kQ, NC, 0, true>(s_rec, s_vid, nullptr, nullptr, 0, ns, kQ, tv, xs, ys, zs, q2, o,
+                                                   cen, zero3, slc, dlc);
+          else
+            eval_cell<double, kQ, kQ, NC, 0, false>(s_rec, s_vid, nullptr, nullptr, 0, ns, kQ, tv, xs, ys, zs, q2, o,
+                                                    cen, zero3, slc, dlc);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            part[c] = 0.0;
+#pragma unroll
+            for (int a = 0; a < kQ; ++a) part[c] += wq[a] * slc[c][a];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] += part[c];
+      } else if (upper) {
+        for (int k = 0; k < kSl64Tris * NC; ++k) my_red[k] = 0.0;
+      }
+      if (upper) {
+        // thread t < kSl64Tris * NC adds column t % NC of triangle t / NC over
+        // the 128 target threads in order
+        __syncthreads();
+        const int k = threadIdx.x / NC, c = threadIdx.x - k * NC;
+        if (threadIdx.x < kSl64Tris * NC && k < ns) {
+          const double* rf = s_red + threadIdx.x;
+          double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+#pragma unroll 8
+          for (int t = 0; t < kTT; t += 4) {
+            v0 += rf[(t + 0) * kRow];
+            v1 += rf[(t + 1) * kRow];
+            v2 += rf[(t + 2) * kRow];
+            v3 += rf[(t + 3) * kRow];
+          }
+          md.partial[c * stride + (size_t)tslot * md.nitems + t0 + k] = (v0 + v1) + (v2 + v3);
+        }
+      }
+      __syncthreads();
+    }
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) md.partial[c * stride + (size_t)w.split * md.nitems + ti] = acc[c];
+    }
+  }
+}
+
 }  // namespace
 
 size_t far_sym_smem_bytes(bool fp32, int nsl, int nd)
 {
-  if (nd == 0) return nsl == 1 ? sl_smem_bytes<1>() : nsl == 3 ? sl_smem_bytes<3>() : sl_smem_bytes<4>();
+  if (nd == 0 && fp32) return nsl == 1 ? sl_smem_bytes<1>() : nsl == 3 ? sl_smem_bytes<3>() : sl_smem_bytes<4>();
+  if (nd == 0) return nsl == 1 ? sl64_smem_bytes<1>() : nsl == 3 ? sl64_smem_bytes<3>() : sl64_smem_bytes<4>();
   return fp32 ? kRecBytes + kRedBytes : kRec64Bytes + kRed64Bytes;
 }
 
@@ -893,6 +1094,11 @@ static const void* sym_kernel_fn(bool fp32, int nsl, int nd)
     if (nsl == 1) return (const void*)far_sym_sl_kernel<1>;
     if (nsl == 3) return (const void*)far_sym_sl_kernel<3>;
     if (nsl == 4) return (const void*)far_sym_sl_kernel<4>;
+  }
+  if (nd == 0 && !fp32) {
+    if (nsl == 1) return (const void*)far_sym64_sl_kernel<1>;
+    if (nsl == 3) return (const void*)far_sym64_sl_kernel<3>;
+    if (nsl == 4) return (const void*)far_sym64_sl_kernel<4>;
   }
   return nullptr;
 }

@@ -23,8 +23,8 @@ constexpr size_t kSymMaxSlotBytes = (size_t)1 << 35;
 // Work list of the symmetric plan for nitems = ne target rows (one item per
 // triangle) and ncells cells; returns the number of partial slots per row.
 int far_sym_items(int nitems, int ncells, int cells_per_item, std::vector<WorkItem>& items);
-// Variants with a symmetric kernel: SL+DL (nsl = nd = 1) in FP32 and FP64;
-// SL only with 1, 3 or 4 right-hand sides in FP32.
+// Variants with a symmetric kernel: SL+DL (nsl = nd = 1) and SL only with 1,
+// 3 or 4 right-hand sides, in FP32 and FP64.
 bool far_sym_variant(bool fp32, int nsl, int nd);
 // Dynamic shared memory of one CTA (staged tile + transposed-sum buffer).
 size_t far_sym_smem_bytes(bool fp32, int nsl, int nd);

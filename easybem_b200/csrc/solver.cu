@@ -219,7 +219,8 @@ int SolverPool::rebuild()
   int cols = 1;
   for (auto& s : sys_) cols = std::max(cols, s->col + 1);
   EB_CHECK(batch_inner_.build(ents, opt_.inner_precision == EB_PREC_MIXED, cols, d_eflag_inner_.as<int>()));
-  EB_CHECK(batch_fp64_.build(ents, false, cols, d_eflag_fp64_.as<int>()));
+  // the FP64 residuals take the symmetric kernel on the default engine too
+  EB_CHECK(batch_fp64_.build(ents, false, cols, d_eflag_fp64_.as<int>(), 0, true));
   std::vector<SysDev> tab(S);
   for (int s = 0; s < S; s++) {
     Sys& y = *sys_[s];

@@ -359,9 +359,11 @@ int eb_mesh_get_plan(eb_mesh mesh, int* items_per_sm, int* src_tile, int* nsplit
 #define EB_FAR_CUDA_CORES 0
 #define EB_FAR_TENSOR_CORES 1
 #define EB_FAR_SYMMETRIC 2
-/* EB_FAR_SYMMETRIC for the FP64 fused SL+DL apply too (every unordered pair
- * once in FP64: 7 instead of 13 FP64-pipe operations per pair). Opt-in:
- * the FP64 default stays the plain ordered-pair kernel; get reports
+/* EB_FAR_SYMMETRIC for the FP64 applies too (every unordered pair once in
+ * FP64: 7 instead of 13 FP64-pipe operations per pair for SL+DL, 5 instead
+ * of 10 for the single layer). Opt-in: the FP64 default of the apply entry
+ * points stays the plain ordered-pair kernel (the solver's internal FP64
+ * residuals take the symmetric kernel on the default engine); get reports
  * EB_FAR_SYMMETRIC for an FP64 apply on this engine. */
 #define EB_FAR_SYMMETRIC_ALL 3
 int eb_mesh_set_far_engine(eb_mesh mesh, int engine);

@@ -165,3 +165,38 @@ def test_symmetric_single_layer_columns(gpu_lib, oracle):
                 assert np.array_equal(vv[c], m.apply_sl(t[c], precision="mixed")), (ncols, c)
     for m in ms:
         m.close()
+
+
+def test_symmetric_single_layer_in_fp64(gpu_lib, oracle):
+    """The FP64 single-layer symmetric kernels (the solver's FP64 residuals on
+    the default engine; every FP64 SL apply on EB_FAR_SYMMETRIC_ALL): the FP64
+    bar against the oracle and the plain kernel, and every column of a 3- or
+    4-column batch bitwise equal to the same column alone."""
+    import torch
+    oracle.set_order(4)
+    cases = [meshes.perturbed_icosphere(4, seed=6), meshes.torus(100, 0.3)]
+    ms = [gpu_lib.Mesh(n, e) for n, e in cases]
+    rng = np.random.default_rng(78)
+    for (nodes, elems), m in zip(cases, ms):
+        t = rng.normal(size=elems.shape[0])
+        rows = np.sort(rng.choice(elems.shape[0], 64, replace=False)).astype(np.int32)
+        vo, _ = oracle.apply_rows(nodes, elems, t, np.zeros(nodes.shape[0]), rows)
+        v0 = m.apply_sl(t)  # the plain ordered-pair FP64 kernel
+        m.set_far_engine("sym_all")
+        v = m.apply_sl(t)
+        assert rel_l2(v[rows], vo) < 1e-12 and rel_l2(v, v0) < 1e-13
+        assert np.array_equal(v, m.apply_sl(t))
+    for ncols in (3, 4):
+        ts = [rng.normal(size=(ncols, m.nelems)) for m in ms]
+        d_t = [torch.from_numpy(x).cuda() for x in ts]
+        d_v = [torch.empty_like(x) for x in d_t]
+        bt = gpu_lib.Batch(ms, ncols, "fp64")
+        bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v])
+        torch.cuda.synchronize()
+        bt.close()
+        for m, t, dv in zip(ms, ts, d_v):
+            vv = dv.cpu().numpy()
+            for c in range(ncols):
+                assert np.array_equal(vv[c], m.apply_sl(t[c])), (ncols, c)
+    for m in ms:
+        m.close()
