@@ -687,6 +687,11 @@ def main():
                                    "'fp64' record is the plain ordered-pair FP64 kernel, the FP64 default"},
         "mixed_over_fp64_symmetric": value / value64s,
         "far_engine": args.far_engine,
+        "pair_count_note": ("value counts the apply's ordered quadrature-point pairs (quad_pairs_per_step) per "
+                            "second; the symmetric engine evaluates each unordered pair of two different "
+                            "128-triangle tiles once and adds it to both rows, so it runs about half as many "
+                            "kernel evaluations (the FP64 default and the CUDA-core engine evaluate every "
+                            "ordered pair)"),
         "other_engines": {e: {"ms_per_step": sum(o[0]) / len(o[0]),
                               "far_ms": sum(f for f, _ in o[1]) / len(o[1]),
                               "Gpairs_per_s": pairs / (sum(f for f, _ in o[1]) / len(o[1]) * 1e-3) / 1e9,
