@@ -92,10 +92,9 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     if (sym_) {  // the mesh's symmetric work list and its own zeroed partial slots
       sym_nsplit = far_sym_items(h.nitems, h.ncells, kSymCellsPerItem, sym_items);
       const size_t bytes = sizeof(double) * (size_t)(nsl_ + nd_) * (size_t)sym_nsplit * h.nitems;
-      if (be->sym_partial.bytes < bytes) {
+      if (be->sym_partial.bytes < bytes) {  // no zeroing: the finalize reads only written slots
         be->sym_partial.release();
         EB_CHECK(be->sym_partial.alloc(bytes));
-        EB_CHECK(memset_sync(be->sym_partial.p, 0, bytes));
       }
       desc[e].partial = be->sym_partial.as<double>();
       desc[e].nsplit = sym_nsplit;
@@ -109,6 +108,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     if (sym_) {
       args[e].partial = be->sym_partial.as<double>();
       args[e].nsplit = sym_nsplit;
+      args[e].sym_cells = far_sym_cells_per_item(kSymCellsPerItem);
     }
     poff[e + 1] = poff[e] + (int)(((long long)h.ne * h.Q + kPrepBlock - 1) / kPrepBlock);
     foff[e + 1] = foff[e] + (h.ne + kFinalizeRows - 1) / kFinalizeRows;

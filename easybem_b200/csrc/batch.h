@@ -28,7 +28,7 @@ struct BatchEntry {
   DevBuf tin, vout;     // kBatchCols columns of nelems each (inputs / outputs)
   DevBuf uin, qout;     // DL density [nnodes] and DL output [nelems] (batches with a DL column)
   DevBuf tc_be, tc_charge;  // tensor-core DL operand and charges (tensor-core SL+DL batches)
-  DevBuf sym_partial;       // symmetric SL+DL batches: partial slots (one per tile and row, zeroed once)
+  DevBuf sym_partial;       // symmetric batches: partial slots (one per tile, row and output)
   int index = -1;       // position in the current batch
 };
 

@@ -678,20 +678,21 @@ bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd, bool fp64_internal)
          m->h.nchunk == 1 && sym_slot_bytes(m->h, nsl + nd) <= kSymMaxSlotBytes;
 }
 
-int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd)
+long long mesh_far_slots(const Mesh* m, bool fp32, int nsl, int nd)
 {
   if (sym_eligible(m, fp32, nsl, nd)) {
-    if (m->sym_nsplit > 0) return m->sym_nsplit;
-    std::vector<WorkItem> items;
-    return far_sym_items(m->h.nitems, m->h.ncells, kSymCellsPerItem, items);
+    const int r = far_sym_cells_per_item(kSymCellsPerItem);
+    long long n = 0;
+    for (int s = 0; s < m->h.ne; s++) n += sym_row_slots(s, m->h.ne, r);
+    return n;
   }
-  return m->plan.nsplit;
+  return (long long)m->plan.nsplit * m->h.nitems;
 }
 
-// The symmetric far field: work list once per mesh, zeroed partial slots for
-// the widest variant used so far (grown and zeroed again when a wider one
-// comes), the descriptor once per scratch allocation, then the persistent
-// kernel.
+// The symmetric far field: work list once per mesh, partial slots for the
+// widest variant used so far (grown when a wider one comes; the finalize
+// reads only the slots each row's items write, so they need no zeroing), the
+// descriptor once per scratch allocation, then the persistent kernel.
 static int sym_far_apply(Mesh* m, bool fp32, int nsl, int nd, cudaStream_t st)
 {
   const HostMesh& h = m->h;
@@ -705,7 +706,6 @@ static int sym_far_apply(Mesh* m, bool fp32, int nsl, int nd, cudaStream_t st)
     m->sym_partial.release();
     m->sym_var.desc.release();
     EB_CHECK(m->sym_partial.alloc(bytes));
-    EB_CUDA(cudaMemsetAsync(m->sym_partial.p, 0, bytes, st));
   }
   if (!m->sym_var.desc.p) {
     FarMeshDesc desc = mesh_far_desc(m, true, 1, 1, m->rec.p, m->sym_partial.as<double>());
@@ -838,6 +838,7 @@ int mesh_apply(Mesh* m, int precision, int nsl, int nd, const double* d_t, const
     EB_CHECK(sym_far_apply(m, fp32, nsl, nd, st));
     A.partial = m->sym_partial.as<double>();
     A.nsplit = m->sym_nsplit;
+    A.sym_cells = far_sym_cells_per_item(kSymCellsPerItem);
   } else if (tc_eligible(m, fp32, nsl, nd)) {
     m->sym_used = false;
     EB_CHECK(tc_far_apply(m, st));
@@ -945,8 +946,7 @@ int eb_mesh_finalize_bytes(eb_mesh mesh, long long* bytes)
   // per row: CSR row pointers, per entry column + value + gathered density,
   // the far-field partial sums of both outputs, the two outputs
   long long b = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8);
-  b += 2 * 8LL * eb::mesh_far_nsplit(mesh->m, true, 1, 1) * h.nitems + 2 * 8 * ne + 8 * ne /* trin */ +
-       4 * ne /* iperm */;
+  b += 2 * 8LL * eb::mesh_far_slots(mesh->m, true, 1, 1) + 2 * 8 * ne + 8 * ne /* trin */ + 4 * ne /* iperm */;
   *bytes = b;
   return EB_OK;
 }
@@ -976,7 +976,7 @@ int eb_mesh_near_field_bytes(eb_mesh mesh, long long* spmv_bytes, long long* fol
   if (spmv_bytes) *spmv_bytes = 2 * 4 * (ne + 1) + sl * (4 + 8 + 8) + dl * (4 + 8 + 8) + 2 * 8 * ne;
   // the fold of the far-field partial sums: both outputs' partial slots, the
   // row's normal/area record and its permutation entry
-  if (fold_bytes) *fold_bytes = 2 * 8LL * eb::mesh_far_nsplit(mesh->m, true, 1, 1) * h.nitems + 8 * ne + 4 * ne;
+  if (fold_bytes) *fold_bytes = 2 * 8LL * eb::mesh_far_slots(mesh->m, true, 1, 1) + 8 * ne + 4 * ne;
   return EB_OK;
 }
 

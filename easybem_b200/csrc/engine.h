@@ -137,9 +137,9 @@ struct Mesh {
   Variant tc_var;
   bool tc_static_ready = false;
   bool tc_used = false;  // the last apply ran the tensor-core kernel
-  // symmetric far field (fused FP32 SL+DL, 7-point rule): its own work list
-  // and partial slots (one per target tile and row, zeroed once: slots no
-  // item writes stay zero), descriptor and launch shape
+  // symmetric far field (7-point rule): its own work list and partial slots
+  // (per output, one per target tile and row; the finalize reads only the
+  // slots a row's items write), descriptor and launch shape
   DevBuf sym_items, sym_partial;
   std::vector<WorkItem> sym_items_host;
   int sym_nitems = 0, sym_nsplit = 0;
@@ -175,9 +175,9 @@ bool tc_eligible(const Mesh* m, bool fp32, int nsl, int nd);
 bool sym_eligible(const Mesh* m, bool fp32, int nsl, int nd, bool fp64_internal = false);
 // Device bytes of the symmetric kernels' partial slots for nout outputs.
 size_t sym_slot_bytes(const HostMesh& h, int nout);
-// Partial slots per row of the far field the next apply in `precision` with
-// nsl SL and nd DL columns would fold.
-int mesh_far_nsplit(const Mesh* m, bool fp32, int nsl, int nd);
+// Partial slots (summed over the rows, per output) the finalize of the next
+// apply in `precision` with nsl SL and nd DL columns would fold.
+long long mesh_far_slots(const Mesh* m, bool fp32, int nsl, int nd);
 // The tensor-core distance operand of m (built once, synchronously).
 int ensure_tc_static(Mesh* m);
 // EB_ERR_TIMEOUT (and the flag cleared) if the last tensor-core launch on m

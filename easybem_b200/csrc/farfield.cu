@@ -366,7 +366,7 @@ __device__ __forceinline__ void finalize_row(const ApplyArgs& A, int row_block)
     // far partial sums of row s: slot k of output c at c*stride + offset(k) + s*nchunk
     const size_t stride = (size_t)A.nsplit * A.nitems;
     const double* base = A.partial + (size_t)s * A.nchunk;
-    const int nparts = A.nsplit * A.nchunk;
+    const int nparts = A.sym_cells > 0 ? sym_row_slots(s, A.ne, A.sym_cells) : A.nsplit * A.nchunk;
     int k = lane;
     for (; k + (kFinPipe - 1) * kFinalizeLanes < nparts; k += kFinPipe * kFinalizeLanes) {
       double x[kFinPipe][NO];

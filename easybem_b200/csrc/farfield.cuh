@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "common.h"
+#include "mesh_host.h"
 
 namespace eb {
 
@@ -143,6 +144,21 @@ struct ApplyArgs {
   double* q;             // DL outputs, nd columns of stride qstride
   int qstride;
   const int* active;     // optional: skip this mesh while *active == 0
+  // symmetric far field: source cells per upper work item (0: every row has
+  // nsplit slots); row s of tile T = s / kTT then has T + 1 + (its tile's upper
+  // items) slots, and the rest are never written nor read
+  int sym_cells = 0;
 };
+
+// Partial slots a row of the symmetric plan holds (sorted row s, ne rows,
+// cells_per_item cells per upper item): one per earlier tile, the diagonal,
+// one per upper item of its own tile.
+__host__ __device__ inline int sym_row_slots(int s, int ne, int cells_per_item)
+{
+  const int t = s / kTT;
+  const int ncells = (ne + kCell - 1) / kCell;
+  const int c0 = (t + 1) * (kTT / kCell);
+  return t + 1 + (c0 < ncells ? (ncells - c0 + cells_per_item - 1) / cells_per_item : 0);
+}
 
 }  // namespace eb

@@ -1129,10 +1129,12 @@ int far_sym_occupancy(bool fp32, int nsl, int nd)
   return occ;
 }
 
+int far_sym_cells_per_item(int cells_per_item) { return std::max(2, (cells_per_item > 0 ? cells_per_item : EB_SYM_CELLS) & ~1); }
+
 int far_sym_items(int nitems, int ncells, int cells_per_item, std::vector<WorkItem>& items)
 {
   const int ntt = (nitems + kTT - 1) / kTT;
-  const int r = std::max(2, (cells_per_item > 0 ? cells_per_item : EB_SYM_CELLS) & ~1);
+  const int r = far_sym_cells_per_item(cells_per_item);
   items.clear();
   int nsplit = 0;
   std::vector<WorkItem> diag;

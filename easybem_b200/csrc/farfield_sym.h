@@ -20,8 +20,11 @@ constexpr int kSymCellsPerItem = 0;
 // 524,288 triangles
 constexpr size_t kSymMaxSlotBytes = (size_t)1 << 35;
 
+// Source cells per upper work item for a requested count (0: the build's default).
+int far_sym_cells_per_item(int cells_per_item);
 // Work list of the symmetric plan for nitems = ne target rows (one item per
-// triangle) and ncells cells; returns the number of partial slots per row.
+// triangle) and ncells cells; returns the largest number of partial slots of
+// a row (sym_row_slots gives each row's).
 int far_sym_items(int nitems, int ncells, int cells_per_item, std::vector<WorkItem>& items);
 // Variants with a symmetric kernel: SL+DL (nsl = nd = 1) and SL only with 1,
 // 3 or 4 right-hand sides, in FP32 and FP64.
