@@ -90,7 +90,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     std::vector<WorkItem> sym_items;
     int sym_nsplit = 0;
     if (sym_) {  // the mesh's symmetric work list and its own zeroed partial slots
-      sym_nsplit = far_sym_items(h.nitems, h.ncells, kSymCellsPerItem, sym_items);
+      sym_nsplit = far_sym_items(h.nitems, h.ncells, kSymBatchCellsPerItem, sym_items);
       const size_t bytes = sizeof(double) * (size_t)(nsl_ + nd_) * (size_t)sym_nsplit * h.nitems;
       if (be->sym_partial.bytes < bytes) {  // no zeroing: the finalize reads only written slots
         be->sym_partial.release();
@@ -108,7 +108,7 @@ int Batch::build(const std::vector<BatchEntry*>& entries, bool fp32, int nsl, in
     if (sym_) {
       args[e].partial = be->sym_partial.as<double>();
       args[e].nsplit = sym_nsplit;
-      args[e].sym_cells = far_sym_cells_per_item(kSymCellsPerItem);
+      args[e].sym_cells = far_sym_cells_per_item(kSymBatchCellsPerItem);
     }
     poff[e + 1] = poff[e] + (int)(((long long)h.ne * h.Q + kPrepBlock - 1) / kPrepBlock);
     foff[e + 1] = foff[e] + (h.ne + kFinalizeRows - 1) / kFinalizeRows;

@@ -15,6 +15,10 @@ constexpr int kSymRule = 7;  // the engine's quadrature rule size (index 4)
 // source cells per upper work item: 0 takes the build's default (8 cells,
 // 256 source triangles)
 constexpr int kSymCellsPerItem = 0;
+// the same in a batch: coarser items keep the merged work list short (many
+// meshes share each launch, and the list is rebuilt whenever the solver's
+// systems change)
+constexpr int kSymBatchCellsPerItem = 32;
 // largest slot allocation the symmetric engine takes (one FP64 value per
 // output, 128-triangle tile and row): 2^35 bytes (32 GiB), an SL+DL mesh of
 // 524,288 triangles
