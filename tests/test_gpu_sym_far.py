@@ -134,7 +134,6 @@ def test_symmetric_single_layer_columns(gpu_lib, oracle):
     the solver's batched applies): against the oracle and the ordered-pair
     kernel, and every column of a 3- or 4-column batch bitwise equal to the
     same column applied alone."""
-    import torch
     oracle.set_order(4)
     cases = [meshes.perturbed_icosphere(4, seed=5), meshes.torus(100, 0.3)]
     v, f = meshes.icosphere(3)
@@ -151,20 +150,34 @@ def test_symmetric_single_layer_columns(gpu_lib, oracle):
         vs = m.apply_sl(t, precision="mixed")
         assert rel_l2(vs[rows], vo) < MIXED_TOL and rel_l2(vs, vc) < MIXED_TOL
         assert np.array_equal(vs, m.apply_sl(t, precision="mixed"))
-    for ncols in (3, 4):
-        ts = [rng.normal(size=(ncols, m.nelems)) for m in ms]
-        d_t = [torch.from_numpy(x).cuda() for x in ts]
-        d_v = [torch.empty_like(x) for x in d_t]
-        bt = gpu_lib.Batch(ms, ncols, "mixed")
-        bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v])
-        torch.cuda.synchronize()
-        bt.close()
-        for m, t, dv in zip(ms, ts, d_v):
-            vv = dv.cpu().numpy()
-            for c in range(ncols):
-                assert np.array_equal(vv[c], m.apply_sl(t[c], precision="mixed")), (ncols, c)
+    _columns_alone_and_together(gpu_lib, ms, rng, "mixed", 1e-12)
     for m in ms:
         m.close()
+
+
+def _batch_apply(gpu_lib, ms, ts, precision):
+    import torch
+    d_t = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in ts]
+    d_v = [torch.empty_like(x) for x in d_t]
+    bt = gpu_lib.Batch(ms, ts[0].shape[0], precision)
+    bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v])
+    torch.cuda.synchronize()
+    bt.close()
+    return [x.cpu().numpy() for x in d_v]
+
+
+def _columns_alone_and_together(gpu_lib, ms, rng, precision, tol):
+    """Every column of a 3- or 4-column batch is bitwise the column applied in
+    a 1-column batch, and agrees with the single-mesh apply (whose work items
+    are finer: the same pairs, summed in other groups) to rounding."""
+    for ncols in (3, 4):
+        ts = [rng.normal(size=(ncols, m.nelems)) for m in ms]
+        vs = _batch_apply(gpu_lib, ms, ts, precision)
+        for c in range(ncols):
+            alone = _batch_apply(gpu_lib, ms, [t[c:c + 1] for t in ts], precision)
+            for m, t, v, a in zip(ms, ts, vs, alone):
+                assert np.array_equal(v[c], a[0]), (ncols, c)
+                assert rel_l2(v[c], m.apply_sl(t[c], precision=precision)) <= tol, (ncols, c)
 
 
 def test_symmetric_single_layer_in_fp64(gpu_lib, oracle):
@@ -172,7 +185,6 @@ def test_symmetric_single_layer_in_fp64(gpu_lib, oracle):
     the default engine; every FP64 SL apply on EB_FAR_SYMMETRIC_ALL): the FP64
     bar against the oracle and the plain kernel, and every column of a 3- or
     4-column batch bitwise equal to the same column alone."""
-    import torch
     oracle.set_order(4)
     cases = [meshes.perturbed_icosphere(4, seed=6), meshes.torus(100, 0.3)]
     ms = [gpu_lib.Mesh(n, e) for n, e in cases]
@@ -186,17 +198,6 @@ def test_symmetric_single_layer_in_fp64(gpu_lib, oracle):
         v = m.apply_sl(t)
         assert rel_l2(v[rows], vo) < 1e-12 and rel_l2(v, v0) < 1e-13
         assert np.array_equal(v, m.apply_sl(t))
-    for ncols in (3, 4):
-        ts = [rng.normal(size=(ncols, m.nelems)) for m in ms]
-        d_t = [torch.from_numpy(x).cuda() for x in ts]
-        d_v = [torch.empty_like(x) for x in d_t]
-        bt = gpu_lib.Batch(ms, ncols, "fp64")
-        bt.apply_device([x.data_ptr() for x in d_t], [x.data_ptr() for x in d_v])
-        torch.cuda.synchronize()
-        bt.close()
-        for m, t, dv in zip(ms, ts, d_v):
-            vv = dv.cpu().numpy()
-            for c in range(ncols):
-                assert np.array_equal(vv[c], m.apply_sl(t[c])), (ncols, c)
+    _columns_alone_and_together(gpu_lib, ms, rng, "fp64", 1e-14)
     for m in ms:
         m.close()
