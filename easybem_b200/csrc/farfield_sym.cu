@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(kTT, 2)
 // every NC, so a column's sums are the same bits alone or among 3 or 4.
 constexpr int kSlPairs = kCell / 2;  // source-triangle pairs per staged cell
 template <int NC>
-__host__ __device__ constexpr int sl_red_stride() { return kSlPairs * NC + 2; }  // float2 per thread row (padded)
+__host__ __device__ constexpr int sl_red_stride() { return kSlPairs * NC + 1; }  // float2 per thread row (odd: conflict-free 8-byte stores)
 template <int NC>
 __host__ __device__ constexpr size_t sl_smem_bytes()
 {
