@@ -41,6 +41,8 @@ _SIGNATURES = {
     "eb_far_engine_costs": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_double)]),
     "eb_mesh_cell_pairs": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "eb_sym_plan": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.c_void_p, ctypes.c_void_p]),
     "eb_set_device_topology_min": (ctypes.c_int, [ctypes.c_int]),
     "eb_get_device_topology_min": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     "eb_mesh_topology_on_device": (ctypes.c_int, [_dp, ctypes.POINTER(ctypes.c_int)]),

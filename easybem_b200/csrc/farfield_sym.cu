@@ -1155,3 +1155,29 @@ int far_sym_items(int nitems, int ncells, int cells_per_item, std::vector<WorkIt
 }
 
 }  // namespace eb
+
+// ---------------------------------------------------------------------------
+// C ABI: the symmetric plan's work list and slot counts (host only).
+
+extern "C" int eb_sym_plan(int nelems, int cells_per_item, int* nitems, int* nslots_max, int* items, int* row_slots)
+{
+  using namespace eb;
+  if (nelems < 1 || cells_per_item < 0) return set_error(EB_ERR_INVALID, "need nelems >= 1 and cells_per_item >= 0");
+  const int ncells = (nelems + kCell - 1) / kCell;
+  std::vector<WorkItem> list;
+  const int nsplit = far_sym_items(nelems, ncells, cells_per_item, list);
+  if (nitems) *nitems = (int)list.size();
+  if (nslots_max) *nslots_max = nsplit;
+  if (items)
+    for (size_t k = 0; k < list.size(); k++) {
+      items[4 * k] = list[k].tgt0;
+      items[4 * k + 1] = list[k].cell0;
+      items[4 * k + 2] = list[k].cell1;
+      items[4 * k + 3] = list[k].split;
+    }
+  if (row_slots) {
+    const int r = far_sym_cells_per_item(cells_per_item);
+    for (int s = 0; s < nelems; s++) row_slots[s] = sym_row_slots(s, nelems, r);
+  }
+  return EB_OK;
+}

@@ -373,6 +373,17 @@ int eb_mesh_get_far_engine(eb_mesh mesh, int precision, int* engine);
  * roots, FMA-pipe lane operations (an FMA counts once) and tensor-core
  * flops (the numerators of the kernels' rooflines). */
 int eb_far_engine_costs(int engine, double* mufu_per_pair, double* fma_ops_per_pair, double* tensor_flops_per_pair);
+/* The symmetric engine's work list for a mesh of nelems triangles in sorted
+ * order (host only, no GPU): *nitems work items as (first target row, first
+ * source cell, end source cell, forward slot) quadruples in items[4 * k ..]
+ * (cells of 32 triangles, target tiles of 128 rows; a source range after the
+ * tile is evaluated in both orders and its transposed sums go to the tile's
+ * slot, a range on the tile itself in forward order), the largest slot count
+ * of a row in *nslots_max, and in row_slots[s] the slots row s holds (the
+ * ones its finalize folds). cells_per_item 0 takes the single-mesh default,
+ * 32 is the batches'. Pass null arrays to get the sizes. No counterpart in
+ * the reference. */
+int eb_sym_plan(int nelems, int cells_per_item, int* nitems, int* nslots_max, int* items, int* row_slots);
 
 /* Times candidate plans (items_per_sm in {4,8,...,512} x source tile in
  * {default, 32, 16}) on this mesh with CUDA events, median of `reps` applies
